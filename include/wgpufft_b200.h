@@ -1,0 +1,187 @@
+/*
+ * wgpufft_b200 — C ABI of the B200 (sm_100a) FFT transform path.
+ *
+ * Drop-in boundary for the public plan API of the Rust crate wgpu-fft
+ * (MaximEremenko/wgpuFFT): every entry point below names the crate function
+ * it replaces (file:line in that project).  wgpu handles become CUDA ones:
+ * a `wgpu::Buffer` becomes a device pointer plus its size in bytes, a
+ * `wgpu::CommandEncoder` becomes a CUDA stream (`cudaStream_t` passed as
+ * `void*`; NULL is the legacy default stream), and `queue.submit` becomes the
+ * stream's own ordering.  Plans record work onto the caller's stream and
+ * return without synchronising, as the crate's plans record into the
+ * caller's encoder (src/plan.rs:494-518).
+ *
+ * Layout conventions are the crate's: interleaved complex values
+ * ([re, im] for f32/f64, [re_hi, re_lo, im_hi, im_lo] f32 words for df64),
+ * axis 0 contiguous, batches as contiguous blocks, real transforms' packed
+ * spectrum [N0/2 + 1, N1, ...] (README.md:111-128, src/math/mod.rs:444-448).
+ *
+ * Errors: every fallible call returns a b2f_status whose values mirror the
+ * crate's FftError variants (src/error.rs:12-177); b2f_last_error_message()
+ * gives the detail of the calling thread's last failure.  Nothing panics or
+ * throws across the ABI.
+ *
+ * Threading: a plan is immutable after creation and may be executed from
+ * several threads on different streams at once, except that the in-place
+ * real-transform copy buffer is created on first use under a lock.
+ */
+#ifndef WGPUFFT_B200_H
+#define WGPUFFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t b2f_status;
+
+/* Status codes (src/error.rs:12-177 variant in brackets). */
+#define B2F_OK 0
+#define B2F_ERR_ZERO_LENGTH 1              /* FftError::ZeroLength */
+#define B2F_ERR_ZERO_BATCH 2               /* FftError::ZeroBatch */
+#define B2F_ERR_LENGTH_TOO_LARGE 3         /* FftError::LengthTooLarge */
+#define B2F_ERR_UNSUPPORTED_LENGTH 4       /* FftError::UnsupportedLength */
+#define B2F_ERR_PRECISION_UNSUPPORTED 5    /* FftError::PrecisionUnsupported */
+#define B2F_ERR_INVALID_TUNING 6           /* FftError::InvalidTuning */
+#define B2F_ERR_EMPTY_AXES 7               /* FftError::EmptyAxes */
+#define B2F_ERR_INVALID_AXIS 8             /* FftError::InvalidAxis */
+#define B2F_ERR_DUPLICATE_AXIS 9           /* FftError::DuplicateAxis */
+#define B2F_ERR_INVALID_REAL_DIRECTION 10  /* FftError::InvalidRealTransformDirection */
+#define B2F_ERR_UNSUPPORTED_REAL_AXES 11   /* FftError::UnsupportedRealAxes */
+#define B2F_ERR_BUFFER_TOO_SMALL 12        /* FftError::BufferViewTooSmall */
+#define B2F_ERR_IN_PLACE_UNSUPPORTED 13    /* FftError::InPlaceUnsupported */
+#define B2F_ERR_RESOURCE_ALLOCATION 14     /* FftError::GpuPlanResourceAllocationFailed */
+#define B2F_ERR_INVALID_ARGUMENT 15        /* null handle or pointer (Rust references cannot be null) */
+#define B2F_ERR_DEVICE 16                  /* a CUDA call failed (wgpu validation/device error) */
+#define B2F_ERR_WORKSPACE_TOO_SMALL 17     /* FftError::WorkspaceTooSmall */
+
+/* FftDirection (src/config.rs:43-57). */
+#define B2F_FORWARD 0
+#define B2F_INVERSE 1
+/* Normalization (src/config.rs:61-71); the crate's default is INVERSE. */
+#define B2F_NORM_NONE 0
+#define B2F_NORM_FORWARD 1
+#define B2F_NORM_INVERSE 2
+#define B2F_NORM_ORTHOGONAL 3
+/* FftPrecision (src/config.rs:6-38). */
+#define B2F_F32 0
+#define B2F_F64 1
+#define B2F_DF64 2
+/* FftTransformKind. */
+#define B2F_C2C 0
+#define B2F_R2C 1
+#define B2F_C2R 2
+
+typedef struct b2f_config b2f_config;
+typedef struct b2f_plan b2f_plan;
+typedef struct b2f_recorder b2f_recorder;
+
+/* ------------------------------------------------------------ FftConfig */
+
+/* FftConfig::new_nd (src/config.rs:90-103): every axis, batch 1, forward,
+ * Normalization::Inverse, f32, default tuning. */
+b2f_status b2f_config_new(b2f_config** out, const uint64_t* shape, uint32_t rank);
+void b2f_config_free(b2f_config* cfg);
+/* FftConfig::with_axes (src/config.rs:122). */
+b2f_status b2f_config_set_axes(b2f_config* cfg, const uint32_t* axes, uint32_t count);
+/* FftConfig::with_batch (src/config.rs:127). */
+b2f_status b2f_config_set_batch(b2f_config* cfg, uint64_t batch);
+/* FftConfig::with_direction (src/config.rs:112). */
+b2f_status b2f_config_set_direction(b2f_config* cfg, int32_t direction);
+/* FftConfig::with_normalization (src/config.rs:117). */
+b2f_status b2f_config_set_normalization(b2f_config* cfg, int32_t normalization);
+/* FftConfig::with_precision (src/config.rs:132). */
+b2f_status b2f_config_set_precision(b2f_config* cfg, int32_t precision);
+/* FftTuning::with_<key> (src/tuning.rs:177-268) for the scalar knobs:
+ * workgroup_size, fused_workgroup_size, rader_max_prime, direct_max_prime,
+ * fused_min_convolution_length, fuse_long_axes, fuse_small_volumes,
+ * large_chunk_max_batches, grouped_batch, swap_to_2_stage_4_step,
+ * swap_to_3_stage_4_step, segmented_burst_depth,
+ * max_storage_buffer_binding_size, max_buffer_size (0 = None for the
+ * optional ones), large_route (0 auto, 1 force-chunk, 2 force-four-step,
+ * 3 force-segmented); and the B200 knobs lines_per_block (0 = planner's
+ * choice), threads_per_block (0 = planner's choice), twiddle_table (1 =
+ * stage twiddles from an FP64-built table, 0 = computed in-kernel). */
+b2f_status b2f_config_set_tuning(b2f_config* cfg, const char* key, int64_t value);
+/* FftTuning::with_force_rader_axes / with_force_bluestein_axes
+ * (src/tuning.rs:197-205): key "force_rader_axes" or "force_bluestein_axes". */
+b2f_status b2f_config_set_tuning_axes(b2f_config* cfg, const char* key, const uint32_t* axes,
+                                      uint32_t count);
+/* FftConfig::validate (src/config.rs:178-211). */
+b2f_status b2f_config_validate(const b2f_config* cfg);
+/* FftConfig::required_buffer_size_bytes (src/config.rs:255-260). */
+b2f_status b2f_config_required_buffer_size_bytes(const b2f_config* cfg, uint64_t* out);
+/* FftConfig::scale / scale_f64 (src/config.rs:262-286). */
+b2f_status b2f_config_scale(const b2f_config* cfg, float* out_f32, double* out_f64);
+
+/* -------------------------------------------------------------- FftPlan */
+
+/* FftPlan::c2c / r2c / c2r (src/plan.rs:221, 327, 355).  The plan binds to
+ * CUDA device `device` (-1 = the calling thread's current device), builds
+ * its tables and workspace there and keeps them until b2f_plan_free. */
+b2f_status b2f_plan_c2c(b2f_plan** out, const b2f_config* cfg, int32_t device);
+b2f_status b2f_plan_r2c(b2f_plan** out, const b2f_config* cfg, int32_t device);
+b2f_status b2f_plan_c2r(b2f_plan** out, const b2f_config* cfg, int32_t device);
+void b2f_plan_free(b2f_plan* plan);
+
+/* FftPlan::kind (src/plan.rs:390): B2F_C2C, B2F_R2C or B2F_C2R. */
+int32_t b2f_plan_kind(const b2f_plan* plan);
+/* FftPlan::required_buffer_size_bytes and the input/output forms
+ * (src/plan.rs:462-484). */
+uint64_t b2f_plan_required_buffer_size_bytes(const b2f_plan* plan);
+uint64_t b2f_plan_required_input_buffer_size_bytes(const b2f_plan* plan);
+uint64_t b2f_plan_required_output_buffer_size_bytes(const b2f_plan* plan);
+/* FftPlan::workspace_size_bytes (src/plan.rs:446): device memory the plan
+ * holds for multi-pass routes (allocated by the plan). */
+uint64_t b2f_plan_workspace_size_bytes(const b2f_plan* plan);
+/* FftPlan::supports_in_place (src/plan.rs:815). */
+int32_t b2f_plan_supports_in_place(const b2f_plan* plan);
+
+/* FftPlan::execute_checked (src/plan.rs:510-518): transform `in` into `out`
+ * on `stream`.  The input buffer is left unchanged. */
+b2f_status b2f_plan_execute_checked(const b2f_plan* plan, void* stream, const void* in,
+                                    uint64_t in_bytes, void* out, uint64_t out_bytes);
+/* FftPlan::execute_in_place (src/plan.rs:827-835). */
+b2f_status b2f_plan_execute_in_place(const b2f_plan* plan, void* stream, void* buffer,
+                                     uint64_t bytes);
+/* FftPlan::diagnostics (src/plan.rs:938-1003) as JSON: route, axis kinds,
+ * factors, stages (label, kind, route, radix schedule, launch shape),
+ * buffer requirements and requested/effective tuning.  On entry *len is the
+ * capacity of buf; on return it is the length needed (without the NUL). */
+b2f_status b2f_plan_diagnostics_json(const b2f_plan* plan, char* buf, uint64_t* len);
+
+/* ---------------------------------------------------------- FftRecorder */
+
+/* FftRecorder::new (src/plan.rs:72-83): starts capturing the work of the
+ * following record calls on `stream` into one CUDA graph, the B200
+ * counterpart of the crate's shared compute pass. */
+b2f_status b2f_recorder_begin(b2f_recorder** out, void* stream);
+/* FftPlan::record (src/plan.rs:882-895). */
+b2f_status b2f_plan_record(const b2f_plan* plan, b2f_recorder* rec, const void* in,
+                           uint64_t in_bytes, void* out, uint64_t out_bytes);
+/* FftPlan::record_in_place (src/plan.rs:839-879). */
+b2f_status b2f_plan_record_in_place(const b2f_plan* plan, b2f_recorder* rec, void* buffer,
+                                    uint64_t bytes);
+/* Ends the capture and instantiates the graph (the crate's encoder.finish). */
+b2f_status b2f_recorder_finish(b2f_recorder* rec);
+/* Launches the recorded graph on `stream` (the crate's queue.submit). */
+b2f_status b2f_recorder_submit(b2f_recorder* rec, void* stream);
+void b2f_recorder_free(b2f_recorder* rec);
+
+/* --------------------------------------------------------------- errors */
+
+/* FftError's Display (src/error.rs): a fixed name for each status. */
+const char* b2f_status_string(b2f_status status);
+/* Detail of the calling thread's last failure; returns its length and
+ * copies at most len-1 bytes plus a NUL into buf (buf may be NULL). */
+uint64_t b2f_last_error_message(char* buf, uint64_t len);
+/* Library version string. */
+const char* b2f_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WGPUFFT_B200_H */

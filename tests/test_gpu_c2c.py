@@ -1,0 +1,165 @@
+"""GPU parity of the complex transforms, through the C ABI, against the FP64
+oracle: every codelet radix, mixed lengths, Rader primes, Bluestein lengths,
+long axes (four-step), N-D shapes and axis subsets, all normalisations,
+forward and inverse, f32 / f64 / df64, in place and out of place, and the
+recorder.  Case lists follow the reference's tests/gpu_c2c.rs, gpu_f64.rs,
+gpu_df64.rs, gpu_accuracy.rs and gpu_long_axes.rs."""
+import numpy as np
+import pytest
+
+import wgpufft_b200 as w
+from oracle import oracle as O
+from tests.gpu_util import TOL, check_c2c, from_device, run_c2c, signal, to_device
+
+pytestmark = pytest.mark.gpu
+
+F32, F64, DF64 = w.FftPrecision.F32, w.FftPrecision.F64, w.FftPrecision.Df64
+INV = w.FftDirection.Inverse
+
+
+@pytest.mark.parametrize("n", list(range(2, 22)) + [32, 49, 64, 100, 121, 128, 169, 243, 256,
+                                                     360, 512, 1000, 1024, 2048, 3003, 4096,
+                                                     8192])
+def test_f32_mixed_radix_lengths(cuda, n):
+    check_c2c(w.FftConfig.new(n).with_batch(3))
+    check_c2c(w.FftConfig.new(n).with_batch(2).with_direction(INV), seed=1)
+
+
+@pytest.mark.parametrize("p", [17, 29, 31, 127, 1009, 2003, 4099, 6121, 8209])
+def test_f32_prime_lengths(cuda, p):
+    check_c2c(w.FftConfig.new(p).with_batch(2), seed=p)
+    check_c2c(w.FftConfig.new(p).with_direction(INV), seed=p + 1)
+
+
+@pytest.mark.parametrize("n", [34, 46, 58, 3256, 10001, 20000])
+def test_f32_bluestein_lengths(cuda, n):
+    check_c2c(w.FftConfig.new(n).with_batch(2), seed=n)
+    check_c2c(w.FftConfig.new(n).with_direction(INV), seed=n + 1)
+
+
+@pytest.mark.parametrize("n", [15015, 16384, 65536, 1 << 20])
+def test_f32_long_axes(cuda, n):
+    check_c2c(w.FftConfig.new(n).with_batch(2), seed=3)
+    check_c2c(w.FftConfig.new(n).with_direction(INV), seed=4)
+
+
+@pytest.mark.parametrize("shape,axes", [([8, 29, 34], None), ([8, 29, 34], [2, 0]),
+                                        ([64, 32], None), ([32, 64], [1]), ([12, 25, 2], None),
+                                        ([5, 7, 9], [1, 2]), ([256, 16384], [1]),
+                                        ([3, 8192], [1]), ([129, 256, 4], None)])
+def test_f32_nd_and_axis_subsets(cuda, shape, axes):
+    cfg = w.FftConfig.new_nd(shape).with_batch(2)
+    if axes is not None:
+        cfg = cfg.with_axes(axes)
+    check_c2c(cfg, seed=5)
+    check_c2c(cfg.with_direction(INV), seed=6)
+
+
+@pytest.mark.parametrize("norm", list(w.Normalization))
+def test_normalisations(cuda, norm):
+    for d in (w.FftDirection.Forward, INV):
+        check_c2c(w.FftConfig.new_nd([16, 12]).with_normalization(norm).with_direction(d), seed=2)
+
+
+def test_length_one(cuda):
+    check_c2c(w.FftConfig.new(1))
+    check_c2c(w.FftConfig.new(1).with_direction(INV))
+
+
+def test_known_length_four(cuda):
+    # src/math/mod.rs:575-612
+    import torch
+    x = np.array([1, 2, 3, 4], dtype=np.complex64)
+    t = torch.from_numpy(x.view(np.float32)).cuda()
+    out = torch.empty_like(t)
+    w.FftPlan.c2c(w.FftConfig.new(4).with_normalization(w.Normalization.NONE)).execute_checked(t, out)
+    got = from_device(out, F32)
+    assert np.max(np.abs(got - np.array([10, -2 + 2j, -2, -2 - 2j]))) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [F64, DF64])
+@pytest.mark.parametrize("n", [2, 3, 5, 7, 11, 13, 16, 17, 100, 1000, 1009, 3000, 3256, 4096,
+                               2999, 65536])
+def test_extended_precision_lengths(cuda, prec, n):
+    check_c2c(w.FftConfig.new(n).with_batch(2).with_precision(prec), seed=11)
+    check_c2c(w.FftConfig.new(n).with_direction(INV).with_precision(prec), seed=12)
+
+
+@pytest.mark.parametrize("prec", [F64, DF64])
+def test_extended_precision_nd(cuda, prec):
+    check_c2c(w.FftConfig.new_nd([12, 25, 2]).with_precision(prec), seed=13)
+    check_c2c(w.FftConfig.new_nd([8, 29, 34]).with_precision(prec).with_direction(INV), seed=14)
+
+
+@pytest.mark.parametrize("prec", [F64, DF64])
+def test_extended_precision_2_20_batch_16(cuda, prec):
+    # the precision configuration: 1D N = 2^20, batch 16
+    check_c2c(w.FftConfig.new(1 << 20).with_batch(16).with_precision(prec), seed=8)
+
+
+@pytest.mark.parametrize("shape,prec", [([1024], F32), ([8, 29, 34], F32), ([15015], F32),
+                                        ([1 << 20], F32), ([4099], F32), ([1000], F64),
+                                        ([4096], DF64)])
+def test_in_place_equals_out_of_place(cuda, shape, prec):
+    cfg = w.FftConfig.new_nd(shape).with_batch(2).with_precision(prec)
+    x = signal(cfg.total_complex_len(), 21)
+    a, _, _ = run_c2c(cfg, x, in_place=False)
+    b, _, _ = run_c2c(cfg, x, in_place=True)
+    assert O.rel_l2(b, a) <= (1e-6 if prec == F32 else 1e-13)
+
+
+def test_recorder_equals_separate_executions(cuda):
+    import torch
+    cfgs = [w.FftConfig.new(1024).with_batch(8), w.FftConfig.new_nd([64, 64]),
+            w.FftConfig.new(1009).with_batch(3)]
+    plans = [w.FftPlan.c2c(c) for c in cfgs]
+    ins, outs_sep, outs_rec = [], [], []
+    for i, c in enumerate(cfgs):
+        t, _ = to_device(signal(c.total_complex_len(), 30 + i), F32)
+        ins.append(t)
+        outs_sep.append(torch.empty_like(t))
+        outs_rec.append(torch.empty_like(t))
+    for p, a, b in zip(plans, ins, outs_sep):
+        p.execute_checked(a, b)
+    torch.cuda.synchronize()
+    rec = w.FftRecorder()
+    for p, a, b in zip(plans, ins, outs_rec):
+        p.record(rec, a, b)
+    rec.submit()
+    rec.submit()
+    torch.cuda.synchronize()
+    for a, b in zip(outs_sep, outs_rec):
+        assert torch.equal(a, b)
+
+
+def test_buffer_too_small_is_reported(cuda):
+    import torch
+    plan = w.FftPlan.c2c(w.FftConfig.new(1024).with_batch(4))
+    small = torch.empty(1024 * 2, dtype=torch.float32, device="cuda")
+    big = torch.empty(1024 * 8, dtype=torch.float32, device="cuda")
+    with pytest.raises(w.FftError) as e:
+        plan.execute_checked(small, big)
+    assert e.value.kind == "BufferViewTooSmall"
+    with pytest.raises(w.FftError) as e:
+        plan.execute_in_place(small)
+    assert e.value.kind == "BufferViewTooSmall"
+
+
+def test_forced_routes_agree(cuda):
+    # forced Rader / Bluestein on the same prime give the same transform
+    x = signal(2 * 127, 40)
+    cfg = w.FftConfig.new(127).with_batch(2)
+    a, exact, _ = run_c2c(cfg, x)
+    b, _, p = run_c2c(cfg.with_tuning(w.FftTuning().with_force_bluestein_axes([0])), x)
+    assert p.axis_kinds() == ["bluestein"]
+    ref = O.c2c_nd_f64(exact, [127], batch=2)
+    assert O.rel_l2(a, ref) < 2e-6 and O.rel_l2(b, ref) < 2e-6
+
+
+def test_computed_twiddles_match_table(cuda):
+    x = signal(4 * 4096, 41)
+    cfg = w.FftConfig.new(4096).with_batch(4)
+    a, exact, _ = run_c2c(cfg, x)
+    b, _, _ = run_c2c(cfg.with_tuning(w.FftTuning().with_twiddle_table(False)), x)
+    ref = O.c2c_nd_f64(exact, [4096], batch=4)
+    assert O.rel_l2(a, ref) < 2e-6 and O.rel_l2(b, ref) < 2e-6

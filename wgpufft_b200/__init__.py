@@ -1,0 +1,544 @@
+"""wgpufft_b200: the FFT transform path of the wgpu-fft crate
+(MaximEremenko/wgpuFFT), rebuilt for NVIDIA B200 (sm_100a).
+
+This module mirrors the crate's public plan API (src/plan.rs, src/config.rs,
+src/tuning.rs) over the C ABI of ``libwgpufft_b200.so``
+(``include/wgpufft_b200.h``):
+
+    cfg = FftConfig.new(1024).with_batch(512)
+    plan = FftPlan.c2c(cfg)                 # FftPlan::c2c (src/plan.rs:221)
+    plan.execute_checked(inp, out)          # src/plan.rs:510
+    plan.execute_in_place(buf)              # src/plan.rs:827
+    with FftRecorder() as rec:              # FftRecorder (src/plan.rs:68-95)
+        plan.record(rec, inp, out)
+    rec.submit()
+
+wgpu buffers become CUDA device memory: a torch CUDA tensor, or an
+``(address, nbytes)`` pair.  There is no CPU fallback: without the built
+library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import json
+import os
+from typing import Iterable, Optional, Sequence, Tuple, Union
+
+__all__ = [
+    "FftDirection", "Normalization", "FftPrecision", "FftTransformKind", "FftTuning",
+    "FftConfig", "FftPlan", "FftRecorder", "FftError", "lib", "library_path",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libwgpufft_b200.so")
+_lib = None
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libwgpufft_b200.so (built by wgpufft_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise FftError("LibraryMissing", 0,
+                           f"{_LIB_PATH} is not built; run python wgpufft_b200/build.py")
+        L = ctypes.CDLL(_LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L: ctypes.CDLL) -> None:
+    vp, u64, i32, u32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32
+    pvp = ctypes.POINTER(ctypes.c_void_p)
+    st = ctypes.c_int32
+    sig = {
+        "b2f_config_new": (st, [pvp, ctypes.POINTER(u64), u32]),
+        "b2f_config_free": (None, [vp]),
+        "b2f_config_set_axes": (st, [vp, ctypes.POINTER(u32), u32]),
+        "b2f_config_set_batch": (st, [vp, u64]),
+        "b2f_config_set_direction": (st, [vp, i32]),
+        "b2f_config_set_normalization": (st, [vp, i32]),
+        "b2f_config_set_precision": (st, [vp, i32]),
+        "b2f_config_set_tuning": (st, [vp, ctypes.c_char_p, ctypes.c_int64]),
+        "b2f_config_set_tuning_axes": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u32), u32]),
+        "b2f_config_validate": (st, [vp]),
+        "b2f_config_required_buffer_size_bytes": (st, [vp, ctypes.POINTER(u64)]),
+        "b2f_config_scale": (st, [vp, ctypes.POINTER(ctypes.c_float),
+                                  ctypes.POINTER(ctypes.c_double)]),
+        "b2f_plan_c2c": (st, [pvp, vp, i32]),
+        "b2f_plan_r2c": (st, [pvp, vp, i32]),
+        "b2f_plan_c2r": (st, [pvp, vp, i32]),
+        "b2f_plan_free": (None, [vp]),
+        "b2f_plan_kind": (i32, [vp]),
+        "b2f_plan_required_buffer_size_bytes": (u64, [vp]),
+        "b2f_plan_required_input_buffer_size_bytes": (u64, [vp]),
+        "b2f_plan_required_output_buffer_size_bytes": (u64, [vp]),
+        "b2f_plan_workspace_size_bytes": (u64, [vp]),
+        "b2f_plan_supports_in_place": (i32, [vp]),
+        "b2f_plan_execute_checked": (st, [vp, vp, vp, u64, vp, u64]),
+        "b2f_plan_execute_in_place": (st, [vp, vp, vp, u64]),
+        "b2f_plan_diagnostics_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_recorder_begin": (st, [pvp, vp]),
+        "b2f_plan_record": (st, [vp, vp, vp, u64, vp, u64]),
+        "b2f_plan_record_in_place": (st, [vp, vp, vp, u64]),
+        "b2f_recorder_finish": (st, [vp]),
+        "b2f_recorder_submit": (st, [vp, vp]),
+        "b2f_recorder_free": (None, [vp]),
+        "b2f_status_string": (ctypes.c_char_p, [st]),
+        "b2f_last_error_message": (u64, [ctypes.c_char_p, u64]),
+        "b2f_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class FftError(Exception):
+    """FftError (src/error.rs:12-177): `kind` is the variant name."""
+
+    def __init__(self, kind: str, code: int, message: str):
+        super().__init__(f"{kind}: {message}")
+        self.kind = kind
+        self.code = code
+        self.message = message
+
+
+def _check(status: int) -> None:
+    if status == 0:
+        return
+    L = lib()
+    kind = L.b2f_status_string(status).decode()
+    buf = ctypes.create_string_buffer(4096)
+    L.b2f_last_error_message(buf, 4096)
+    raise FftError(kind, status, buf.value.decode())
+
+
+class FftDirection(enum.IntEnum):
+    """FftDirection (src/config.rs:43-57)."""
+    Forward = 0
+    Inverse = 1
+
+
+class Normalization(enum.IntEnum):
+    """Normalization (src/config.rs:61-71); default Inverse."""
+    NONE = 0
+    Forward = 1
+    Inverse = 2
+    Orthogonal = 3
+
+
+class FftPrecision(enum.IntEnum):
+    """FftPrecision (src/config.rs:6-38)."""
+    F32 = 0
+    F64 = 1
+    Df64 = 2
+
+    def as_str(self) -> str:
+        return ("f32", "f64", "df64")[int(self)]
+
+    def scalar_size_bytes(self) -> int:
+        return 4 if self == FftPrecision.F32 else 8
+
+    def complex_size_bytes(self) -> int:
+        return 2 * self.scalar_size_bytes()
+
+
+class FftTransformKind(enum.IntEnum):
+    C2c = 0
+    R2c = 1
+    C2r = 2
+
+
+_SCALAR_TUNING = (
+    "workgroup_size", "fused_workgroup_size", "rader_max_prime", "direct_max_prime",
+    "large_route", "large_chunk_max_batches", "grouped_batch", "swap_to_2_stage_4_step",
+    "swap_to_3_stage_4_step", "segmented_burst_depth", "max_storage_buffer_binding_size",
+    "max_buffer_size", "fused_min_convolution_length", "fuse_long_axes", "fuse_small_volumes",
+    "lines_per_block", "threads_per_block", "twiddle_table",
+)
+_TUNING_DEFAULTS = {
+    "workgroup_size": 64, "fused_workgroup_size": 256, "rader_max_prime": 8192,
+    "direct_max_prime": 127, "large_route": 0, "large_chunk_max_batches": None,
+    "grouped_batch": None, "swap_to_2_stage_4_step": 0, "swap_to_3_stage_4_step": 0,
+    "segmented_burst_depth": 2, "max_storage_buffer_binding_size": None,
+    "max_buffer_size": None, "fused_min_convolution_length": 128, "fuse_long_axes": True,
+    "fuse_small_volumes": True, "lines_per_block": 0, "threads_per_block": 0,
+    "twiddle_table": True,
+}
+
+
+class FftTuning:
+    """FftTuning (src/tuning.rs:35-268): immutable builder; `with_<knob>`
+    returns a copy.  Adds the B200 launch knobs lines_per_block,
+    threads_per_block (0 = planner's choice) and twiddle_table."""
+
+    def __init__(self, **values):
+        self._v = dict(_TUNING_DEFAULTS)
+        self._v["force_rader_axes"] = []
+        self._v["force_bluestein_axes"] = []
+        for k, v in values.items():
+            if k not in self._v:
+                raise AttributeError(k)
+            self._v[k] = v
+
+    def __getattr__(self, name):
+        if name.startswith("with_"):
+            key = name[5:]
+            if key in self._v:
+                def setter(value):
+                    t = FftTuning()
+                    t._v = dict(self._v)
+                    t._v[key] = list(value) if key.startswith("force_") else value
+                    return t
+                return setter
+        if name in ("_v",):
+            raise AttributeError(name)
+        if name in self._v:
+            return self._v[name]
+        raise AttributeError(name)
+
+    def __eq__(self, other):
+        return isinstance(other, FftTuning) and self._v == other._v
+
+    def as_dict(self):
+        return dict(self._v)
+
+
+class FftConfig:
+    """FftConfig (src/config.rs:75-286): immutable builder."""
+
+    def __init__(self, shape: Sequence[int], axes: Optional[Sequence[int]] = None, batch: int = 1,
+                 direction: FftDirection = FftDirection.Forward,
+                 normalization: Normalization = Normalization.Inverse,
+                 precision: FftPrecision = FftPrecision.F32,
+                 tuning: Optional[FftTuning] = None):
+        self._shape = [int(s) for s in shape]
+        self._axes = list(range(len(self._shape))) if axes is None else [int(a) for a in axes]
+        self._batch = int(batch)
+        self._direction = FftDirection(direction)
+        self._normalization = Normalization(normalization)
+        self._precision = FftPrecision(precision)
+        self._tuning = tuning if tuning is not None else FftTuning()
+
+    # constructors (src/config.rs:86-110)
+    @classmethod
+    def new(cls, length: int) -> "FftConfig":
+        return cls([length])
+
+    @classmethod
+    def new_nd(cls, shape: Sequence[int]) -> "FftConfig":
+        return cls(shape)
+
+    @classmethod
+    def inverse(cls, length: int) -> "FftConfig":
+        return cls([length], direction=FftDirection.Inverse)
+
+    @classmethod
+    def inverse_nd(cls, shape: Sequence[int]) -> "FftConfig":
+        return cls(shape, direction=FftDirection.Inverse)
+
+    def _copy(self, **kw) -> "FftConfig":
+        d = dict(shape=self._shape, axes=self._axes, batch=self._batch,
+                 direction=self._direction, normalization=self._normalization,
+                 precision=self._precision, tuning=self._tuning)
+        d.update(kw)
+        return FftConfig(**d)
+
+    def with_direction(self, d) -> "FftConfig":
+        return self._copy(direction=d)
+
+    def with_normalization(self, n) -> "FftConfig":
+        return self._copy(normalization=n)
+
+    def with_axes(self, axes) -> "FftConfig":
+        return self._copy(axes=list(axes))
+
+    def with_batch(self, b) -> "FftConfig":
+        return self._copy(batch=b)
+
+    def with_precision(self, p) -> "FftConfig":
+        return self._copy(precision=p)
+
+    def with_tuning(self, t: FftTuning) -> "FftConfig":
+        return self._copy(tuning=t)
+
+    def shape(self):
+        return list(self._shape)
+
+    def axes(self):
+        return list(self._axes)
+
+    def batch(self):
+        return self._batch
+
+    def direction(self):
+        return self._direction
+
+    def normalization(self):
+        return self._normalization
+
+    def precision(self):
+        return self._precision
+
+    def tuning(self):
+        return self._tuning
+
+    def __len__(self):
+        return self._shape[0] if self._shape else 0
+
+    def __eq__(self, other):
+        return isinstance(other, FftConfig) and self.__dict__ == other.__dict__
+
+    def _handle(self) -> "_ConfigHandle":
+        return _ConfigHandle(self)
+
+    def validate(self) -> None:
+        with self._handle() as h:
+            _check(lib().b2f_config_validate(h.ptr))
+
+    def total_complex_len(self) -> int:
+        n = self._batch
+        for s in self._shape:
+            n *= s
+        return n
+
+    def required_buffer_size_bytes(self) -> int:
+        with self._handle() as h:
+            out = ctypes.c_uint64()
+            _check(lib().b2f_config_required_buffer_size_bytes(h.ptr, ctypes.byref(out)))
+            return out.value
+
+    def scale(self) -> float:
+        with self._handle() as h:
+            f, d = ctypes.c_float(), ctypes.c_double()
+            _check(lib().b2f_config_scale(h.ptr, ctypes.byref(f), ctypes.byref(d)))
+            return f.value
+
+    def scale_f64(self) -> float:
+        with self._handle() as h:
+            f, d = ctypes.c_float(), ctypes.c_double()
+            _check(lib().b2f_config_scale(h.ptr, ctypes.byref(f), ctypes.byref(d)))
+            return d.value
+
+
+class _ConfigHandle:
+    """A b2f_config built from an FftConfig for the duration of one call."""
+
+    def __init__(self, cfg: FftConfig):
+        L = lib()
+        self.ptr = ctypes.c_void_p()
+        shape = (ctypes.c_uint64 * len(cfg._shape))(*cfg._shape)
+        _check(L.b2f_config_new(ctypes.byref(self.ptr), shape, len(cfg._shape)))
+        axes = (ctypes.c_uint32 * max(1, len(cfg._axes)))(*[a & 0xFFFFFFFF for a in cfg._axes])
+        _check(L.b2f_config_set_axes(self.ptr, axes, len(cfg._axes)))
+        _check(L.b2f_config_set_batch(self.ptr, cfg._batch & 0xFFFFFFFFFFFFFFFF))
+        _check(L.b2f_config_set_direction(self.ptr, int(cfg._direction)))
+        _check(L.b2f_config_set_normalization(self.ptr, int(cfg._normalization)))
+        _check(L.b2f_config_set_precision(self.ptr, int(cfg._precision)))
+        for k in _SCALAR_TUNING:
+            v = cfg._tuning._v[k]
+            v = 0 if v is None else int(v)
+            _check(L.b2f_config_set_tuning(self.ptr, k.encode(), v))
+        for k in ("force_rader_axes", "force_bluestein_axes"):
+            ax = cfg._tuning._v[k]
+            arr = (ctypes.c_uint32 * max(1, len(ax)))(*ax)
+            _check(L.b2f_config_set_tuning_axes(self.ptr, k.encode(), arr, len(ax)))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        lib().b2f_config_free(self.ptr)
+        self.ptr = None
+
+
+Buffer = Union["torch.Tensor", Tuple[int, int]]  # noqa: F821
+
+
+def _buf(b) -> Tuple[int, int]:
+    if isinstance(b, tuple):
+        return int(b[0]), int(b[1])
+    if hasattr(b, "data_ptr"):
+        if not b.is_cuda:
+            raise FftError("InvalidArgument", 15, "buffers must be CUDA device memory")
+        return int(b.data_ptr()), int(b.numel() * b.element_size())
+    raise TypeError("buffer must be a torch CUDA tensor or an (address, nbytes) pair")
+
+
+def _stream(s) -> int:
+    if s is None:
+        try:
+            import torch
+            return int(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return 0
+    if isinstance(s, int):
+        return s
+    return int(s.cuda_stream)
+
+
+class FftPlan:
+    """FftPlan (src/plan.rs:32-1300)."""
+
+    def __init__(self, ptr: ctypes.c_void_p, config: FftConfig, kind: FftTransformKind):
+        self._ptr = ptr
+        self._config = config
+        self._kind = kind
+        self._diag = None
+
+    @classmethod
+    def _make(cls, fn, config: FftConfig, device: Optional[int], kind) -> "FftPlan":
+        L = lib()
+        p = ctypes.c_void_p()
+        dev = -1 if device is None else int(device)
+        with config._handle() as h:
+            _check(getattr(L, fn)(ctypes.byref(p), h.ptr, dev))
+        return cls(p, config, kind)
+
+    @classmethod
+    def c2c(cls, config: FftConfig, device: Optional[int] = None) -> "FftPlan":
+        return cls._make("b2f_plan_c2c", config, device, FftTransformKind.C2c)
+
+    @classmethod
+    def r2c(cls, config: FftConfig, device: Optional[int] = None) -> "FftPlan":
+        return cls._make("b2f_plan_r2c", config, device, FftTransformKind.R2c)
+
+    @classmethod
+    def c2r(cls, config: FftConfig, device: Optional[int] = None) -> "FftPlan":
+        return cls._make("b2f_plan_c2r", config, device, FftTransformKind.C2r)
+
+    @classmethod
+    def plan_only(cls, config: FftConfig, kind: FftTransformKind = FftTransformKind.C2c
+                  ) -> "FftPlan":
+        """Runs the planner without a device (diagnostics only; cannot execute)."""
+        fn = {0: "b2f_plan_c2c", 1: "b2f_plan_r2c", 2: "b2f_plan_c2r"}[int(kind)]
+        return cls._make(fn, config, -2, FftTransformKind(kind))
+
+    def __del__(self):
+        try:
+            if self._ptr:
+                lib().b2f_plan_free(self._ptr)
+                self._ptr = None
+        except Exception:
+            pass
+
+    def close(self):
+        self.__del__()
+
+    # sizes and introspection (src/plan.rs:390-492, 815)
+    def kind(self) -> FftTransformKind:
+        return self._kind
+
+    def config(self) -> FftConfig:
+        return self._config
+
+    def required_buffer_size_bytes(self) -> int:
+        return lib().b2f_plan_required_buffer_size_bytes(self._ptr)
+
+    def required_input_buffer_size_bytes(self) -> int:
+        return lib().b2f_plan_required_input_buffer_size_bytes(self._ptr)
+
+    def required_output_buffer_size_bytes(self) -> int:
+        return lib().b2f_plan_required_output_buffer_size_bytes(self._ptr)
+
+    def workspace_size_bytes(self) -> int:
+        return lib().b2f_plan_workspace_size_bytes(self._ptr)
+
+    def supports_in_place(self) -> bool:
+        return bool(lib().b2f_plan_supports_in_place(self._ptr))
+
+    def packed_shape(self):
+        if self._kind == FftTransformKind.C2c:
+            return None
+        s = self._config.shape()
+        s[0] = s[0] // 2 + 1
+        return s
+
+    def diagnostics(self) -> dict:
+        if self._diag is None:
+            L = lib()
+            n = ctypes.c_uint64(0)
+            _check(L.b2f_plan_diagnostics_json(self._ptr, None, ctypes.byref(n)))
+            buf = ctypes.create_string_buffer(n.value + 1)
+            n2 = ctypes.c_uint64(n.value + 1)
+            _check(L.b2f_plan_diagnostics_json(self._ptr, buf, ctypes.byref(n2)))
+            self._diag = json.loads(buf.value.decode())
+        return self._diag
+
+    def route(self) -> str:
+        return self.diagnostics()["route"]
+
+    def axis_kinds(self):
+        return self.diagnostics()["axis_kinds"]
+
+    def axis_factors(self):
+        return self.diagnostics()["axis_factors"]
+
+    def factors(self):
+        f = self.axis_factors()
+        return f[0] if f else []
+
+    # execution (src/plan.rs:494-879)
+    def execute_checked(self, input: Buffer, output: Buffer, stream=None) -> None:
+        ip, ib = _buf(input)
+        op, ob = _buf(output)
+        _check(lib().b2f_plan_execute_checked(self._ptr, _stream(stream), ip, ib, op, ob))
+
+    def execute(self, input: Buffer, output: Buffer, stream=None) -> None:
+        """FftPlan::execute (src/plan.rs:494): the crate panics on invalid
+        buffers; here the FftError propagates."""
+        self.execute_checked(input, output, stream)
+
+    def execute_in_place(self, buffer: Buffer, stream=None) -> None:
+        bp, bb = _buf(buffer)
+        _check(lib().b2f_plan_execute_in_place(self._ptr, _stream(stream), bp, bb))
+
+    def record(self, recorder: "FftRecorder", input: Buffer, output: Buffer) -> None:
+        ip, ib = _buf(input)
+        op, ob = _buf(output)
+        _check(lib().b2f_plan_record(self._ptr, recorder._ptr, ip, ib, op, ob))
+
+    def record_in_place(self, recorder: "FftRecorder", buffer: Buffer) -> None:
+        bp, bb = _buf(buffer)
+        _check(lib().b2f_plan_record_in_place(self._ptr, recorder._ptr, bp, bb))
+
+
+class FftRecorder:
+    """FftRecorder (src/plan.rs:68-95): records several plans' work into one
+    CUDA graph; `submit` launches it (the crate's queue.submit)."""
+
+    def __init__(self, stream=None):
+        self._ptr = ctypes.c_void_p()
+        _check(lib().b2f_recorder_begin(ctypes.byref(self._ptr), _stream(stream)))
+        self._finished = False
+
+    def finish(self) -> "FftRecorder":
+        if not self._finished:
+            self._finished = True
+            _check(lib().b2f_recorder_finish(self._ptr))
+        return self
+
+    def submit(self, stream=None) -> None:
+        self.finish()
+        _check(lib().b2f_recorder_submit(self._ptr, _stream(stream)))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        if exc_type is None:
+            self.finish()
+
+    def __del__(self):
+        try:
+            if self._ptr:
+                lib().b2f_recorder_free(self._ptr)
+                self._ptr = None
+        except Exception:
+            pass

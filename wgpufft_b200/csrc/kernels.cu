@@ -1,0 +1,128 @@
+// Precision dispatch of the kernel launchers; the kernels themselves are
+// instantiated once per precision in kernels_f32.cu, kernels_f64.cu and
+// kernels_df64.cu (compiled in parallel).
+#include <mutex>
+
+#include "kernels.h"
+
+namespace b2f {
+
+template <class S>
+cudaError_t launch_lines_t(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
+template <class S>
+cudaError_t launch_rader_t(const RaderParams&, unsigned, unsigned, size_t, cudaStream_t);
+template <class S>
+cudaError_t launch_bluestein_t(const BluesteinParams&, unsigned, unsigned, size_t, cudaStream_t);
+template <class S>
+cudaError_t launch_r2c_t(const RealParams&, unsigned, unsigned, size_t, cudaStream_t);
+template <class S>
+cudaError_t launch_c2r_t(const RealParams&, unsigned, unsigned, size_t, cudaStream_t);
+template <class S>
+cudaError_t launch_scale_copy_t(const void*, void*, uint64_t, double, bool, cudaStream_t);
+template <class S>
+cudaError_t launch_blue_elem_t(const BlueElemParams&, cudaStream_t);
+
+cudaError_t launch_blue_elem(Prec p, const BlueElemParams& prm, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_blue_elem_t<float>(prm, st);
+    case PREC_F64: return launch_blue_elem_t<double>(prm, st);
+    case PREC_DF64: return launch_blue_elem_t<df>(prm, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+static size_t g_max_smem = 0;
+
+size_t max_smem_per_block() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      v = 48 * 1024;
+    g_max_smem = (size_t)v;
+  });
+  return g_max_smem;
+}
+
+template <class S, int E, bool COLMAJOR>
+cudaError_t launch_pow2_t(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
+
+cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
+                        unsigned threads, size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32:
+      if (E == 32)
+        return colmajor ? launch_pow2_t<float, 32, true>(prm, grid, threads, smem, st)
+                        : launch_pow2_t<float, 32, false>(prm, grid, threads, smem, st);
+      return colmajor ? launch_pow2_t<float, 16, true>(prm, grid, threads, smem, st)
+                      : launch_pow2_t<float, 16, false>(prm, grid, threads, smem, st);
+    case PREC_F64:
+      return colmajor ? launch_pow2_t<double, 16, true>(prm, grid, threads, smem, st)
+                      : launch_pow2_t<double, 16, false>(prm, grid, threads, smem, st);
+    case PREC_DF64:
+      return colmajor ? launch_pow2_t<df, 16, true>(prm, grid, threads, smem, st)
+                      : launch_pow2_t<df, 16, false>(prm, grid, threads, smem, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_lines(Prec p, const LinesParams& prm, unsigned grid, unsigned threads,
+                         size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_lines_t<float>(prm, grid, threads, smem, st);
+    case PREC_F64: return launch_lines_t<double>(prm, grid, threads, smem, st);
+    case PREC_DF64: return launch_lines_t<df>(prm, grid, threads, smem, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rader(Prec p, const RaderParams& prm, unsigned grid, unsigned threads,
+                         size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_rader_t<float>(prm, grid, threads, smem, st);
+    case PREC_F64: return launch_rader_t<double>(prm, grid, threads, smem, st);
+    case PREC_DF64: return launch_rader_t<df>(prm, grid, threads, smem, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_bluestein(Prec p, const BluesteinParams& prm, unsigned grid,
+                             unsigned threads, size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_bluestein_t<float>(prm, grid, threads, smem, st);
+    case PREC_F64: return launch_bluestein_t<double>(prm, grid, threads, smem, st);
+    case PREC_DF64: return launch_bluestein_t<df>(prm, grid, threads, smem, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_r2c(Prec p, const RealParams& prm, unsigned grid, unsigned threads,
+                       size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_r2c_t<float>(prm, grid, threads, smem, st);
+    case PREC_F64: return launch_r2c_t<double>(prm, grid, threads, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_c2r(Prec p, const RealParams& prm, unsigned grid, unsigned threads,
+                       size_t smem, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_c2r_t<float>(prm, grid, threads, smem, st);
+    case PREC_F64: return launch_c2r_t<double>(prm, grid, threads, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_scale_copy(Prec p, const void* in, void* out, uint64_t n, double scale,
+                              bool conj, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_scale_copy_t<float>(in, out, n, scale, conj, st);
+    case PREC_F64: return launch_scale_copy_t<double>(in, out, n, scale, conj, st);
+    case PREC_DF64: return launch_scale_copy_t<df>(in, out, n, scale, conj, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace b2f

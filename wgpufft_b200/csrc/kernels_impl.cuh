@@ -1,0 +1,548 @@
+// Transform kernels for sm_100a.  Each kernel stages G lines of one pass in
+// shared memory, runs the Stockham engine (engine.cuh) and writes the lines
+// back, fusing everything a pass needs around the FFT into the same trip
+// through HBM: conjugation for inverse transforms, the four-step twiddle,
+// normalisation, the Rader permutations and kernel-spectrum product, the
+// Bluestein chirps, and the real-to-complex packing.
+#pragma once
+#include <mutex>
+#include <set>
+#include <utility>
+
+#include "kernels.h"
+
+namespace b2f {
+
+template <class S>
+using C = cpx<S>;
+
+struct Group {
+  int64_t in0, out0, dl_in, dl_out;
+  uint32_t nvalid;
+  uint64_t c0;
+};
+
+FFT_D Group group_of(const LineIO& io, uint32_t G, uint64_t blk) {
+  Group g;
+  const uint64_t rest = blk / io.tiles;
+  const uint64_t tile = blk - rest * io.tiles;
+  const uint64_t outer = rest / io.mid_n;
+  const uint64_t mid = rest - outer * io.mid_n;
+  const uint64_t c0 = tile * G;
+  const uint64_t left = io.inner_n - c0;
+  g.nvalid = left < G ? (uint32_t)left : G;
+  g.in0 = (int64_t)outer * io.in_outer + (int64_t)mid * io.in_mid + (int64_t)c0 * io.in_inner;
+  g.out0 = (int64_t)outer * io.out_outer + (int64_t)mid * io.out_mid + (int64_t)c0 * io.out_inner;
+  g.dl_in = io.in_inner;
+  g.dl_out = io.out_inner;
+  g.c0 = c0;
+  return g;
+}
+
+// Visits the (line c, point n) pairs of a G x count block.  cfirst walks
+// adjacent lines first (coalesced when lines are adjacent columns); else it
+// walks each line's points first (coalesced when lines are contiguous).
+template <class F>
+FFT_D void for_each_elem(uint32_t count, const FastDiv& dcount, uint32_t G, const FastDiv& dG,
+                         bool cfirst, uint32_t tid, uint32_t T, F f) {
+  const uint32_t total = G * count;
+  if (cfirst) {
+    for (uint32_t e = tid; e < total; e += T) {
+      const uint32_t n = fdiv(e, dG);
+      f(e - n * G, n);
+    }
+  } else {
+    for (uint32_t e = tid; e < total; e += T) {
+      const uint32_t c = fdiv(e, dcount);
+      f(c, e - c * count);
+    }
+  }
+}
+
+template <class S>
+FFT_D void load_lines(C<S>* sm, const LinesParams& p, const Group& g, uint32_t tid, uint32_t T) {
+  constexpr int PAD = PadOf<S>::value;
+  const C<S>* __restrict__ in = (const C<S>*)p.in;
+  const bool conj_in = p.flags & PF_CONJ_IN;
+  for_each_elem(p.N, p.dN, p.G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T,
+                [&](uint32_t c, uint32_t n) {
+                  if (c < g.nvalid) {
+                    C<S> v = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
+                    if (conj_in) v.im = -v.im;
+                    sm[c * p.LD + pidx<PAD>(n)] = v;
+                  }
+                });
+}
+
+template <class S>
+FFT_D void store_lines(const C<S>* sm, const LinesParams& p, const Group& g, uint32_t tid,
+                       uint32_t T) {
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const uint32_t fl = p.flags;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(p.N, p.dN, p.G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < g.nvalid) {
+      C<S> v = sm[c * p.LD + pidx<PAD>(n)];
+      if (fl & PF_TW_STORE) {
+        const uint64_t row = fdiv((uint32_t)(g.c0 + c), p.d_tw);
+        const uint64_t m = (row * (uint64_t)n) % p.tw_store_M;
+        v = cmul(v, twiddle<S>(m, p.tw_store_M));
+      }
+      if (fl & PF_SCALE) v = cscale(v, sc);
+      if (fl & PF_CONJ_OUT) v.im = -v.im;
+      out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
+    }
+  });
+}
+
+template <class S>
+FFT_D const C<S>* tw_of(const LinesParams& p) {
+  return (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr;
+}
+
+// ------------------------------------------------------------ mixed radix
+// Shared memory: two line buffers of G*LD elements (ping-pong).
+template <class S>
+__global__ void __launch_bounds__(512) k_lines(const __grid_constant__ LinesParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const Group g = group_of(p.io, p.G, blockIdx.x);
+  load_lines<S>(A, p, g, tid, T);
+  __syncthreads();
+  const C<S>* res = fft_lines_smem<S>(A, B, p.sch, p.G, p.LD, tid, T, tw_of<S>(p));
+  store_lines<S>(res, p, g, tid, T);
+}
+
+// ------------------------------------------------------------------ Rader
+// X[0] = sum x; X[g^-r] = x[0] + (a (*) b)[r] with a[q] = x[g^q] and
+// b[q] = W_p^{g^-q}, a cyclic convolution of length p-1 taken through
+// FFT_{p-1}, the product with the precomputed spectrum of b, and the
+// inverse FFT (src/runtime/rader_axis.rs:1228-1336 builds the same pieces).
+// Shared memory: two buffers of G*LD, then x0[G] and X0[G].
+template <class S>
+__global__ void __launch_bounds__(512) k_rader(const __grid_constant__ RaderParams rp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  const LinesParams& p = rp.L;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  C<S>* x0s = B + p.G * p.LD;
+  C<S>* X0s = x0s + p.G;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t P = p.N, P1 = P - 1, G = p.G, LD = p.LD;
+  const Group g = group_of(p.io, G, blockIdx.x);
+  load_lines<S>(A, p, g, tid, T);
+  __syncthreads();
+  if (tid < G) x0s[tid] = A[tid * LD];
+  {
+    const uint32_t tot = G * P1;
+    for (uint32_t e = tid; e < tot; e += T) {
+      const uint32_t l = fdiv(e, rp.dP1), q = e - l * P1;
+      B[l * LD + pidx<PAD>(q)] = A[l * LD + pidx<PAD>(rp.perm_in[q])];
+    }
+  }
+  __syncthreads();
+  C<S>* r1 = fft_lines_smem<S>(B, A, p.sch, G, LD, tid, T, tw_of<S>(p));
+  C<S>* o1 = (r1 == A) ? B : A;
+  if (tid < G) X0s[tid] = x0s[tid] + r1[tid * LD];
+  __syncthreads();
+  {
+    const C<S>* __restrict__ bhat = (const C<S>*)rp.bhat;
+    const uint32_t tot = G * P1;
+    for (uint32_t e = tid; e < tot; e += T) {
+      const uint32_t l = fdiv(e, rp.dP1), m = e - l * P1;
+      C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], bhat[m]);
+      v.im = -v.im;
+      r1[l * LD + pidx<PAD>(m)] = v;
+    }
+  }
+  __syncthreads();
+  const C<S>* r2 = fft_lines_smem<S>(r1, o1, p.sch, G, LD, tid, T, tw_of<S>(p));
+  // X[n] = x0 + conv[r(n)], conv = conj(result)
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const uint32_t fl = p.flags;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(P, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < g.nvalid) {
+      C<S> v;
+      if (n == 0) {
+        v = X0s[c];
+      } else {
+        C<S> w = r2[c * LD + pidx<PAD>(rp.perm_out[n - 1])];
+        w.im = -w.im;
+        v = x0s[c] + w;
+      }
+      if (fl & PF_SCALE) v = cscale(v, sc);
+      if (fl & PF_CONJ_OUT) v.im = -v.im;
+      out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
+    }
+  });
+}
+
+// -------------------------------------------------------------- Bluestein
+// X[k] = c_k * sum_j (x_j c_j) conj(c_{k-j}) with the chirp
+// c_n = exp(-i pi n^2 / N), n^2 reduced modulo 2N in integers
+// (src/runtime/bluestein_axis.rs:825-867); the convolution runs over M >= 2N-1
+// points against the precomputed spectrum of the conjugate chirp.
+template <class S>
+FFT_D C<S> chirp(uint64_t n, uint32_t N) {
+  const uint64_t twoN = 2ull * N;
+  return twiddle<S>((n * n) % twoN, twoN);
+}
+
+template <class S>
+__global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ BluesteinParams bp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  const LinesParams& p = bp.L;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t N = p.N, M = bp.M, G = p.G, LD = p.LD;
+  const Group g = group_of(p.io, G, blockIdx.x);
+  {
+    const C<S>* __restrict__ in = (const C<S>*)p.in;
+    const bool conj_in = p.flags & PF_CONJ_IN;
+    for_each_elem(N, p.dN, G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T, [&](uint32_t c, uint32_t n) {
+      if (c < g.nvalid) {
+        C<S> v = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
+        if (conj_in) v.im = -v.im;
+        A[c * LD + pidx<PAD>(n)] = cmul(v, chirp<S>(n, N));
+      }
+    });
+    const uint32_t pad = M - N;
+    const uint32_t tot = G * pad;
+    for (uint32_t e = tid; e < tot; e += T) {
+      const uint32_t l = fdiv(e, bp.dMN), m = N + (e - l * pad);
+      A[l * LD + pidx<PAD>(m)] = czero<S>();
+    }
+  }
+  __syncthreads();
+  C<S>* r1 = fft_lines_smem<S>(A, B, p.sch, G, LD, tid, T, tw_of<S>(p));
+  C<S>* o1 = (r1 == A) ? B : A;
+  {
+    const C<S>* __restrict__ bhat = (const C<S>*)bp.bhat;
+    const uint32_t tot = G * M;
+    for (uint32_t e = tid; e < tot; e += T) {
+      const uint32_t l = fdiv(e, bp.dM), m = e - l * M;
+      C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], bhat[m]);
+      v.im = -v.im;
+      r1[l * LD + pidx<PAD>(m)] = v;
+    }
+  }
+  __syncthreads();
+  const C<S>* r2 = fft_lines_smem<S>(r1, o1, p.sch, G, LD, tid, T, tw_of<S>(p));
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const uint32_t fl = p.flags;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(N, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t k) {
+    if (c < g.nvalid) {
+      C<S> w = r2[c * LD + pidx<PAD>(k)];
+      w.im = -w.im;
+      C<S> v = cmul(w, chirp<S>(k, N));
+      if (fl & PF_SCALE) v = cscale(v, sc);
+      if (fl & PF_CONJ_OUT) v.im = -v.im;
+      out[g.out0 + (int64_t)c * g.dl_out + (int64_t)k * p.io.out_es] = v;
+    }
+  });
+}
+
+// ------------------------------------------------------------------ real
+// R2C, even N0 = 2h: the real line read as h complex pairs z[n] = x[2n] +
+// i x[2n+1], Z = FFT_h(z), then X[k] = E + W^k O and X[h-k] = conj(E - W^k O)
+// with E = (Z[k] + conj Z[h-k]) / 2, O = -i (Z[k] - conj Z[h-k]) / 2, written
+// straight to the packed layout [N0/2 + 1, ...] of the reference
+// (src/math/mod.rs:444-448).
+template <class S>
+__global__ void __launch_bounds__(512) k_r2c_even(const __grid_constant__ RealParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t h = p.h, G = p.G, LD = p.LD, P = h + 1;
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
+  const C<S>* __restrict__ in = (const C<S>*)p.in;
+  for_each_elem(h, p.dh, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < nvalid) A[c * LD + pidx<PAD>(n)] = in[(l0 + c) * h + n];
+  });
+  __syncthreads();
+  const C<S>* Z = fft_lines_smem<S>(A, B, p.sch, G, LD, tid, T,
+                                     (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr);
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const S half = Scalar<S>::from_double(0.5);
+  const S sc = Scalar<S>::from_double(p.scale);
+  const uint32_t K = h / 2 + 1;
+  const uint32_t tot = G * K;
+  for (uint32_t e = tid; e < tot; e += T) {
+    const uint32_t c = e / K, k = e - c * K;
+    if (c >= nvalid) continue;
+    const C<S> a = Z[c * LD + pidx<PAD>(k)];
+    const C<S> b = conj(Z[c * LD + pidx<PAD>(k == 0 ? 0 : h - k)]);
+    const C<S> E = cscale(a + b, half);
+    const C<S> O = cscale(mul_neg_i(a - b), half);
+    const C<S> WO = cmul(O, twiddle<S>(k, p.N0));
+    C<S> xk = E + WO;
+    C<S> xh = conj(E - WO);
+    if (p.flags & PF_SCALE) {
+      xk = cscale(xk, sc);
+      xh = cscale(xh, sc);
+    }
+    C<S>* line = out + (l0 + c) * P;
+    line[k] = xk;
+    if (h - k != k) line[h - k] = xh;
+  }
+}
+
+// C2R, even N0 = 2h: Z[k] = (X[k] + conj X[h-k]) + i conj(W^k) (X[k] - conj
+// X[h-k]) for k < h (imaginary parts of X[0] and X[h] ignored, as the
+// reference's CPU and GPU routes do, src/cpu.rs:476-481), then an inverse
+// FFT_h gives (x[2n], x[2n+1]) unnormalised.
+template <class S>
+__global__ void __launch_bounds__(512) k_c2r_even(const __grid_constant__ RealParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t h = p.h, G = p.G, LD = p.LD, P = h + 1;
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
+  const C<S>* __restrict__ in = (const C<S>*)p.in;
+  for_each_elem(P, p.dP, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t k) {
+    if (c < nvalid) A[c * LD + pidx<PAD>(k)] = in[(l0 + c) * P + k];
+  });
+  __syncthreads();
+  {
+    const uint32_t K = h / 2 + 1;
+    const uint32_t tot = G * K;
+    for (uint32_t e = tid; e < tot; e += T) {
+      const uint32_t c = e / K, k = e - c * K;
+      C<S> Xk = A[c * LD + pidx<PAD>(k)];
+      C<S> Xh = A[c * LD + pidx<PAD>(h - k)];
+      if (k == 0) {
+        Xk.im = Scalar<S>::zero();
+        Xh.im = Scalar<S>::zero();
+      }
+      const C<S> Pp = Xk + conj(Xh);
+      const C<S> Q = Xk - conj(Xh);
+      const C<S> iWQ = mul_i(cmulc(Q, twiddle<S>(k, p.N0)));  // i conj(W^k) Q
+      // stored conjugated: the forward engine then computes the inverse
+      B[c * LD + pidx<PAD>(k)] = conj(Pp + iWQ);
+      if (k != 0 && h - k != k) B[c * LD + pidx<PAD>(h - k)] = Pp - iWQ;
+    }
+  }
+  __syncthreads();
+  const C<S>* y = fft_lines_smem<S>(B, A, p.sch, G, LD, tid, T,
+                                     (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr);
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(h, p.dh, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < nvalid) {
+      C<S> v = conj(y[c * LD + pidx<PAD>(n)]);
+      if (p.flags & PF_SCALE) v = cscale(v, sc);
+      out[(l0 + c) * h + n] = v;
+    }
+  });
+}
+
+// R2C, odd N0: a complex FFT of the real line, first (N0+1)/2 outputs kept.
+template <class S>
+__global__ void __launch_bounds__(512) k_r2c_odd(const __grid_constant__ RealParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t N0 = p.N0, G = p.G, LD = p.LD, P = N0 / 2 + 1;
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
+  const S* __restrict__ in = (const S*)p.in;
+  for_each_elem(N0, p.dN0, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < nvalid) A[c * LD + pidx<PAD>(n)] = {in[(l0 + c) * N0 + n], Scalar<S>::zero()};
+  });
+  __syncthreads();
+  const C<S>* y = fft_lines_smem<S>(A, B, p.sch, G, LD, tid, T,
+                                     (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr);
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(P, p.dP, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t k) {
+    if (c < nvalid) {
+      C<S> v = y[c * LD + pidx<PAD>(k)];
+      if (p.flags & PF_SCALE) v = cscale(v, sc);
+      out[(l0 + c) * P + k] = v;
+    }
+  });
+}
+
+// C2R, odd N0: the Hermitian line rebuilt in shared memory (imaginary part
+// of X[0] ignored), an inverse complex FFT, the real part kept.
+template <class S>
+__global__ void __launch_bounds__(512) k_c2r_odd(const __grid_constant__ RealParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* A = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* B = A + p.G * p.LD;
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t N0 = p.N0, G = p.G, LD = p.LD, P = N0 / 2 + 1;
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
+  const C<S>* __restrict__ in = (const C<S>*)p.in;
+  for_each_elem(P, p.dP, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t k) {
+    if (c < nvalid) {
+      C<S> X = in[(l0 + c) * P + k];
+      if (k == 0) X.im = Scalar<S>::zero();
+      A[c * LD + pidx<PAD>(k)] = conj(X);  // conjugated input of the inverse
+      if (k != 0) A[c * LD + pidx<PAD>(N0 - k)] = X;
+    }
+  });
+  __syncthreads();
+  const C<S>* y = fft_lines_smem<S>(A, B, p.sch, G, LD, tid, T,
+                                     (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr);
+  S* __restrict__ out = (S*)p.out;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for_each_elem(N0, p.dN0, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t n) {
+    if (c < nvalid) {
+      S v = y[c * LD + pidx<PAD>(n)].re;
+      if (p.flags & PF_SCALE) v = v * sc;
+      out[(l0 + c) * N0 + n] = v;
+    }
+  });
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueElemParams p) {
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t N = p.N, M = p.M;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for (uint64_t l = blockIdx.x; l < p.nlines; l += gridDim.x) {
+    const uint64_t o = l / p.s, i = l - o * p.s;
+    const int64_t base = (int64_t)(o * (uint64_t)N * p.s + i);
+    if (p.mode == BE_PRE) {
+      const C<S>* __restrict__ in = (const C<S>*)p.in;
+      C<S>* __restrict__ ws = (C<S>*)p.out + l * M;
+      for (uint32_t m = tid; m < M; m += T) {
+        C<S> v = czero<S>();
+        if (m < N) {
+          v = in[base + (int64_t)m * (int64_t)p.s];
+          if (p.flags & PF_CONJ_IN) v.im = -v.im;
+          v = cmul(v, chirp<S>(m, N));
+        }
+        ws[m] = v;
+      }
+    } else if (p.mode == BE_MID) {
+      C<S>* ws = (C<S>*)p.out + l * M;
+      const C<S>* __restrict__ bhat = (const C<S>*)p.bhat;
+      for (uint32_t k = tid; k < M; k += T) {
+        C<S> v = cmul(ws[k], bhat[k]);
+        v.im = -v.im;
+        ws[k] = v;
+      }
+    } else {
+      const C<S>* __restrict__ ws = (const C<S>*)p.in + l * M;
+      C<S>* __restrict__ out = (C<S>*)p.out;
+      for (uint32_t k = tid; k < N; k += T) {
+        C<S> w = ws[k];
+        w.im = -w.im;
+        C<S> v = cmul(w, chirp<S>(k, N));
+        if (p.flags & PF_SCALE) v = cscale(v, sc);
+        if (p.flags & PF_CONJ_OUT) v.im = -v.im;
+        out[base + (int64_t)k * (int64_t)p.s] = v;
+      }
+    }
+  }
+}
+
+template <class S>
+__global__ void k_scale_copy(const C<S>* __restrict__ in, C<S>* __restrict__ out, uint64_t n,
+                             double scale, int conj_flag) {
+  const S sc = Scalar<S>::from_double(scale);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    C<S> v = cscale(in[i], sc);
+    if (conj_flag) v.im = -v.im;
+    out[i] = v;
+  }
+}
+
+// --------------------------------------------------- templated launchers
+// Raises the dynamic shared memory limit of a kernel once per (kernel,
+// device); kernels are told apart by address, not by type.
+template <class K>
+static cudaError_t prepare(K kernel, size_t smem) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (smem <= 48 * 1024) return cudaSuccess;
+  const std::pair<const void*, int> key((const void*)kernel, dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(key)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)max_smem_per_block());
+  if (e == cudaSuccess) done.insert(key);
+  return e;
+}
+
+template <class K, class P>
+static cudaError_t launch(K kernel, const P& prm, unsigned grid, unsigned threads, size_t smem,
+                          cudaStream_t st) {
+  cudaError_t e = prepare(kernel, smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, threads, smem, st>>>(prm);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t launch_lines_t(const LinesParams& prm, unsigned grid, unsigned threads, size_t smem,
+                           cudaStream_t st) {
+  return launch(k_lines<S>, prm, grid, threads, smem, st);
+}
+template <class S>
+cudaError_t launch_rader_t(const RaderParams& prm, unsigned grid, unsigned threads, size_t smem,
+                           cudaStream_t st) {
+  return launch(k_rader<S>, prm, grid, threads, smem, st);
+}
+template <class S>
+cudaError_t launch_bluestein_t(const BluesteinParams& prm, unsigned grid, unsigned threads,
+                               size_t smem, cudaStream_t st) {
+  return launch(k_bluestein<S>, prm, grid, threads, smem, st);
+}
+template <class S>
+cudaError_t launch_r2c_t(const RealParams& prm, unsigned grid, unsigned threads, size_t smem,
+                         cudaStream_t st) {
+  if (prm.N0 % 2 == 0) return launch(k_r2c_even<S>, prm, grid, threads, smem, st);
+  return launch(k_r2c_odd<S>, prm, grid, threads, smem, st);
+}
+template <class S>
+cudaError_t launch_c2r_t(const RealParams& prm, unsigned grid, unsigned threads, size_t smem,
+                         cudaStream_t st) {
+  if (prm.N0 % 2 == 0) return launch(k_c2r_even<S>, prm, grid, threads, smem, st);
+  return launch(k_c2r_odd<S>, prm, grid, threads, smem, st);
+}
+template <class S>
+cudaError_t launch_blue_elem_t(const BlueElemParams& prm, cudaStream_t st) {
+  uint64_t blocks = prm.nlines < 148ull * 16 ? prm.nlines : 148ull * 16;
+  if (blocks == 0) blocks = 1;
+  k_blue_elem<S><<<(unsigned)blocks, 256, 0, st>>>(prm);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t launch_scale_copy_t(const void* in, void* out, uint64_t n, double scale, bool conj,
+                                cudaStream_t st) {
+  const unsigned threads = 256;
+  uint64_t blocks = (n + threads - 1) / threads;
+  if (blocks > 148ull * 32) blocks = 148ull * 32;
+  if (blocks == 0) blocks = 1;
+  k_scale_copy<S><<<(unsigned)blocks, threads, 0, st>>>((const C<S>*)in, (C<S>*)out, n, scale,
+                                                        conj ? 1 : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace b2f
