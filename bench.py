@@ -1,0 +1,424 @@
+"""Benchmark of the FFT transform path on B200.
+
+Headline workload (the configuration the metric is quoted on): 20,000 1D
+complex f32 forward transforms whose lengths are log-uniform in [16, 65536]
+(70% 13-smooth, 15% prime, 15% other composite; seed 5), values iid N(0,1),
+lines stored back to back (1.27 GB in, 1.27 GB out: larger than L2, so no
+flush is needed between steps).  One step = one batched launch over all
+20,000 lines (b2f_batch_execute).  Reported beside it:
+  - plain per-plan: the same lines, one FftPlan per length, one
+    execute_checked per line (what a caller of the reference's plan API does);
+  - e2e: the batched step through the public API with the input copied from
+    pinned host memory and the output copied back inside the timed region;
+  - roofline: the cluster (long-line) kernel alone, achieved algorithmic
+    GB/s (16 B per complex point per transform) against the measured HBM
+    copy bandwidth;
+  - cpu_baseline: the planned CPU FFT (oracle/cpu_port.c, a C restatement of
+    the reference's CpuFftPlan structure) on a bounded sample of the lines.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun every rank runs the whole workload on its own GPU (replicas,
+weak scaling); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mixed-size FFTs/s + p50/p99 latency, served vs plain per-plan, at ≤2e-6 rel L2"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"b2f_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 7:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    mx = float(f[1])
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        except FileNotFoundError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample_rate(lengths, offsets, x, seconds_target=10.0, threads=0):
+    """Planned CPU FFT over a bounded sample of the lines: returns
+    (FFTs/s, lines in the sample, threads)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(11)
+    idx = rng.permutation(len(lengths))
+    # grow the sample until one pass takes ~seconds_target / 3
+    take = 500
+    while True:
+        sel = np.sort(idx[:take])
+        ls = lengths[sel]
+        off = np.zeros(len(ls), dtype=np.int64)
+        off[1:] = np.cumsum(ls[:-1])
+        data = np.empty(int(ls.sum()), dtype=np.complex64)
+        for j, i in enumerate(sel):
+            data[off[j]:off[j] + ls[j]] = x[offsets[i]:offsets[i] + lengths[i]]
+        lines = O.CpuLines(off, ls)
+        lines.run(data.copy(), threads=threads)  # warm-up
+        t0 = time.perf_counter()
+        lines.run(data, threads=threads)
+        dt = time.perf_counter() - t0
+        if dt > seconds_target / 3 or take >= len(lengths):
+            reps = max(1, int(seconds_target / max(dt, 1e-3)) // 2)
+            times = [dt]
+            for _ in range(min(reps, 4)):
+                t0 = time.perf_counter()
+                lines.run(data, threads=threads)
+                times.append(time.perf_counter() - t0)
+            med = statistics.median(times)
+            nthreads = threads if threads > 0 else O.cpu_max_threads()
+            lines.close()
+            return len(sel) / med, len(sel), nthreads, med
+        lines.close()
+        take = min(len(lengths), take * 3)
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's CPU path (the planned CPU port of
+    CpuFftPlan; the reference's Rust crate cannot be built here) on the host
+    cores, a bounded sample of the same workload per step."""
+    from wgpufft_b200 import workloads as W
+    if rank != 0:
+        return
+    lengths = W.mixed_lengths()
+    offsets = W.packed_offsets(lengths)
+    x = W.normal_complex(int(lengths.sum()), 5)
+    rate, nsample, threads, sec = cpu_sample_rate(lengths, offsets, x, seconds_target=6.0)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "FFTs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded), bounded sample",
+        "config": {"workload": "20,000 mixed-length 1D C2C f32 forward lines, log-uniform "
+                               "[16, 65536], seed 5 (CPU: bounded sample)",
+                   "sample_lines": nsample},
+        "cpu_baseline": {"value": rate, "unit": "FFTs/s", "cores": threads, "kind": "port",
+                         "sample": f"{nsample} lines drawn from the 20,000-line workload"},
+        "e2e": {"value": rate, "unit": "FFTs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import wgpufft_b200 as w
+    from wgpufft_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lengths = W.mixed_lengths()
+    offsets = W.packed_offsets(lengths)
+    total = int(lengths.sum())
+    x = W.normal_complex(total, 5)
+    nbytes = total * 8
+    alg_bytes = 2 * nbytes  # one read + one write of every complex point
+    batch = w.FftBatch(lengths, offsets, w.FftDirection.Forward, device=local)
+    diag = batch.diagnostics()
+    dx = torch.from_numpy(x.view(np.float32)).to(dev)
+    dy = torch.empty_like(dx)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- batched launch, data resident in HBM
+    for _ in range(args.warmup):
+        batch.execute(dx, dy)
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.execute(dx, dy)
+            e1.record(stream)
+            step_ms.append((e0, e1))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    total_ms = ev0.elapsed_time(ev1)
+    per_step = [a.elapsed_time(b) for a, b in step_ms]
+    total_ms = max_over_ranks(world, total_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * len(lengths) * args.steps / (total_ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- roofline: the cluster kernel (long lines: most of the bytes) alone
+    cl_lines = lengths[lengths > 0]
+    nd = diag
+    rf = None
+    hbm_peak, peak_kind = load_peaks()
+    try:
+        cl_bytes = 0
+        # lines classified to clusters are the ones the planner reports; recompute
+        # their bytes by running the cluster part alone and timing it
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            batch.execute_parts(dx, dy, 2, sequential=True)
+        torch.cuda.synchronize()
+        a0.record(stream)
+        reps = max(3, args.steps // 2)
+        for _ in range(reps):
+            batch.execute_parts(dx, dy, 2, sequential=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        cl_ms = a0.elapsed_time(a1) / reps
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            batch.execute_parts(dx, dy, 1, sequential=True)
+        torch.cuda.synchronize()
+        b0.record(stream)
+        for _ in range(reps):
+            batch.execute_parts(dx, dy, 1, sequential=True)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        cta_ms = b0.elapsed_time(b1) / reps
+        cl_lens = np.array(nd.get("cluster_line_lengths", []))
+        cl_elems = int(nd.get("cluster_elements", 0))
+        cta_elems = int(nd.get("cta_elements", 0))
+        cl_alg = 16 * cl_elems
+        cta_alg = 16 * cta_elems
+        ach_cl = cl_alg / (cl_ms / 1e3) / 1e9
+        ach_cta = cta_alg / (cta_ms / 1e3) / 1e9
+        rf = {"bound": "hbm", "kernel": "k_batch_cluster<8> (lines too long for one CTA)",
+              "achieved": ach_cl, "peak": hbm_peak, "unit": "GB/s", "frac": ach_cl / hbm_peak,
+              "peak_kind": peak_kind, "traffic": None,
+              "algorithmic_bytes_per_launch": cl_alg, "ms_per_launch": cl_ms,
+              "other_kernel": {"kernel": "k_batch_cta (lines that fit one CTA)",
+                               "achieved": ach_cta, "frac": ach_cta / hbm_peak,
+                               "algorithmic_bytes_per_launch": cta_alg,
+                               "ms_per_launch": cta_ms},
+              "whole_step": {"achieved": alg_bytes / (ms_per_step / 1e3) / 1e9,
+                             "frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}}
+        traffic_file = os.path.join(ROOT, "profiles", "batch_traffic.json")
+        if os.path.exists(traffic_file):
+            with open(traffic_file) as f:
+                rf["traffic"] = json.load(f).get("k_batch_cluster_bytes_per_launch")
+    except Exception as exc:  # measurement must not hide the headline
+        rf = {"bound": "hbm", "error": str(exc)}
+
+    # ---- e2e: pinned host buffers, copies inside the timed region
+    hx = torch.from_numpy(x.view(np.float32)).pin_memory()
+    hy = torch.empty_like(hx).pin_memory()
+    for _ in range(2):
+        dx.copy_(hx, non_blocking=True)
+        batch.execute(dx, dy)
+        hy.copy_(dy, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier(world)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for _ in range(e2e_steps):
+        dx.copy_(hx, non_blocking=True)
+        batch.execute(dx, dy)
+        hy.copy_(dy, non_blocking=True)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, c0.elapsed_time(c1)) / e2e_steps
+    e2e = {"value": world * len(lengths) / (e2e_ms / 1e3), "unit": "FFTs/s",
+           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "ms_per_step": e2e_ms}
+
+    # ---- plain per-plan: one plan per length, one execute per line
+    plain = None
+    if not args.no_plain:
+        plans = {}
+        for n in np.unique(lengths):
+            plans[int(n)] = w.FftPlan.c2c(w.FftConfig.new(int(n)), device=local)
+        base_x, base_y = dx.data_ptr(), dy.data_ptr()
+
+        def plain_step():
+            for n, o in zip(lengths.tolist(), offsets.tolist()):
+                plans[n].execute_checked((base_x + 8 * o, 8 * n), (base_y + 8 * o, 8 * n))
+        plain_step()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        p0.record(stream)
+        plain_steps = 2
+        for _ in range(plain_steps):
+            plain_step()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) / plain_steps
+        pms = p0.elapsed_time(p1) / plain_steps
+        plain = {"value": len(lengths) / (pms / 1e3), "unit": "FFTs/s", "ms_per_step": pms,
+                 "host_wall_ms_per_step": wall * 1e3, "launches_per_step": len(lengths)}
+        del plans
+
+    # ---- accuracy on sampled lines against the FP64 oracle
+    acc = None
+    try:
+        from oracle import oracle as O
+        y = dy.cpu().numpy().view(np.complex64)
+        rng = np.random.default_rng(0)
+        errs = []
+        for i in rng.choice(len(lengths), 16, replace=False):
+            n, o = int(lengths[i]), int(offsets[i])
+            ref = O.fft_f64(x[o:o + n].astype(np.complex128))
+            errs.append(O.rel_l2(y[o:o + n], ref))
+        acc = {"max_rel_l2_sampled": max(errs), "lines": len(errs)}
+    except Exception as exc:
+        acc = {"error": str(exc)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            rate, nsample, threads, sec = cpu_sample_rate(lengths, offsets, x, seconds_target=6.0)
+            cpu = {"value": rate, "unit": "FFTs/s", "cores": threads, "kind": "port",
+                   "sample": f"{nsample} lines drawn from the 20,000-line workload "
+                             f"(planned C port of CpuFftPlan)"}
+        except Exception as exc:
+            cpu = {"error": str(exc)}
+
+    lat = sorted(per_step)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "FFTs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded N(0,1) complex, lengths drawn per the workload)",
+            "config": {"workload": "20,000 mixed-length 1D C2C f32 forward lines, lengths "
+                                   "log-uniform [16, 65536] (70% 13-smooth / 15% prime / 15% "
+                                   "other), batched persistent launch",
+                       "lines": int(len(lengths)), "distinct_lengths": int(diag["distinct_lengths"]),
+                       "complex_points": total, "bytes_in": nbytes,
+                       "l2": "inputs (1.27 GB) larger than L2; no flush",
+                       "parallelism": f"replicas x{world}"},
+            "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1,
+                                                                        int(len(lat) * 0.99))],
+                        "unit": "ms per 20,000-line batch"},
+            "plain_per_plan": plain,
+            "served_vs_plain": (value / world / plain["value"]) if plain else None,
+            "gflops": world * sum(W.fft_flops(int(n)) for n in lengths) * args.steps
+            / (total_ms / 1e3) / 1e9,
+            "roofline": rf,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "accuracy": acc,
+            "clocks": clocks,
+            "gpu_launches": 2 * args.steps,
+            "batch": diag,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        barrier(world)
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,6 +170,36 @@ b2f_status b2f_recorder_finish(b2f_recorder* rec);
 b2f_status b2f_recorder_submit(b2f_recorder* rec, void* stream);
 void b2f_recorder_free(b2f_recorder* rec);
 
+/* ------------------------------------------------------- batched launch */
+
+/* Many 1D complex f32 transforms of mixed lengths in one persistent launch
+ * (no counterpart in the crate, which records one dispatch chain per plan):
+ * line i has lengths[i] points at complex offset offsets[i] of the input and
+ * output buffers (lines must not overlap); direction and normalization are
+ * shared.  Lines that fit one CTA are taken from a device work queue by
+ * persistent CTAs; longer lines (up to ~100k points, Bluestein lengths up
+ * to ~50k) run on 8-CTA thread-block clusters through distributed shared
+ * memory, one HBM pass each. */
+typedef struct b2f_batch b2f_batch;
+b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
+                         uint64_t count, int32_t direction, int32_t normalization,
+                         int32_t device);
+void b2f_batch_free(b2f_batch* batch);
+/* Bytes each of the input and output buffers must hold. */
+uint64_t b2f_batch_required_buffer_size_bytes(const b2f_batch* batch);
+/* Transforms every line of `in` into `out` (in == out allowed). */
+b2f_status b2f_batch_execute(const b2f_batch* batch, void* stream, const void* in,
+                             uint64_t in_bytes, void* out, uint64_t out_bytes);
+/* b2f_batch_execute restricted to a subset of the lines, for measuring one
+ * kernel alone: parts bit 0 = lines that fit one CTA, bit 1 = cluster lines;
+ * sequential != 0 runs both kernels on `stream` one after the other instead
+ * of overlapping them on two streams. */
+b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const void* in,
+                                   uint64_t in_bytes, void* out, uint64_t out_bytes,
+                                   uint32_t parts, int32_t sequential);
+/* Task and launch summary as JSON (same length convention as the plan's). */
+b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_t* len);
+
 /* --------------------------------------------------------------- errors */
 
 /* FftError's Display (src/error.rs): a fixed name for each status. */

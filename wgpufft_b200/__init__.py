@@ -27,7 +27,7 @@ from typing import Iterable, Optional, Sequence, Tuple, Union
 
 __all__ = [
     "FftDirection", "Normalization", "FftPrecision", "FftTransformKind", "FftTuning",
-    "FftConfig", "FftPlan", "FftRecorder", "FftError", "lib", "library_path",
+    "FftConfig", "FftPlan", "FftRecorder", "FftBatch", "FftError", "lib", "library_path",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -89,6 +89,12 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_recorder_finish": (st, [vp]),
         "b2f_recorder_submit": (st, [vp, vp]),
         "b2f_recorder_free": (None, [vp]),
+        "b2f_batch_new": (st, [pvp, ctypes.POINTER(u64), ctypes.POINTER(u64), u64, i32, i32, i32]),
+        "b2f_batch_free": (None, [vp]),
+        "b2f_batch_required_buffer_size_bytes": (u64, [vp]),
+        "b2f_batch_execute": (st, [vp, vp, vp, u64, vp, u64]),
+        "b2f_batch_diagnostics_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_batch_execute_parts": (st, [vp, vp, vp, u64, vp, u64, u32, i32]),
         "b2f_status_string": (ctypes.c_char_p, [st]),
         "b2f_last_error_message": (u64, [ctypes.c_char_p, u64]),
         "b2f_version": (ctypes.c_char_p, []),
@@ -507,6 +513,56 @@ class FftPlan:
     def record_in_place(self, recorder: "FftRecorder", buffer: Buffer) -> None:
         bp, bb = _buf(buffer)
         _check(lib().b2f_plan_record_in_place(self._ptr, recorder._ptr, bp, bb))
+
+
+class FftBatch:
+    """Many 1D complex f32 lines of mixed lengths in one persistent launch
+    (b2f_batch_*): line i has lengths[i] points at complex offset offsets[i]."""
+
+    def __init__(self, lengths, offsets, direction=FftDirection.Forward,
+                 normalization=Normalization.Inverse, device: Optional[int] = None):
+        L = lib()
+        n = len(lengths)
+        la = (ctypes.c_uint64 * n)(*[int(x) for x in lengths])
+        oa = (ctypes.c_uint64 * n)(*[int(x) for x in offsets])
+        self._ptr = ctypes.c_void_p()
+        _check(L.b2f_batch_new(ctypes.byref(self._ptr), la, oa, n, int(direction),
+                               int(normalization), -1 if device is None else int(device)))
+        self.count = n
+
+    def required_buffer_size_bytes(self) -> int:
+        return lib().b2f_batch_required_buffer_size_bytes(self._ptr)
+
+    def execute(self, input: Buffer, output: Buffer, stream=None) -> None:
+        ip, ib = _buf(input)
+        op, ob = _buf(output)
+        _check(lib().b2f_batch_execute(self._ptr, _stream(stream), ip, ib, op, ob))
+
+    def execute_parts(self, input: Buffer, output: Buffer, parts: int, sequential: bool = False,
+                      stream=None) -> None:
+        """Runs only the CTA-queue lines (parts=1), the cluster lines
+        (parts=2) or both (3)."""
+        ip, ib = _buf(input)
+        op, ob = _buf(output)
+        _check(lib().b2f_batch_execute_parts(self._ptr, _stream(stream), ip, ib, op, ob, parts,
+                                             int(sequential)))
+
+    def diagnostics(self) -> dict:
+        L = lib()
+        n = ctypes.c_uint64(0)
+        _check(L.b2f_batch_diagnostics_json(self._ptr, None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        n2 = ctypes.c_uint64(n.value + 1)
+        _check(L.b2f_batch_diagnostics_json(self._ptr, buf, ctypes.byref(n2)))
+        return json.loads(buf.value.decode())
+
+    def __del__(self):
+        try:
+            if self._ptr:
+                lib().b2f_batch_free(self._ptr)
+                self._ptr = None
+        except Exception:
+            pass
 
 
 class FftRecorder:

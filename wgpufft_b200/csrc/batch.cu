@@ -1,0 +1,606 @@
+// Batched launch of many 1D f32 lines of mixed lengths: host planner and
+// C ABI (b2f_batch_*).  The north-star "batching form": the lines of all the
+// transforms share persistent launches driven by a device work queue; the
+// reference has no counterpart (it records one dispatch chain per plan).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <thread>
+
+#include "batch.cuh"
+#include "hostfft.h"
+#include "plan.h"
+
+namespace b2f {
+
+static bool smooth7(uint64_t n) {
+  if (n == 0) return false;
+  for (uint64_t r : {2, 3, 5, 7})
+    while (n % r == 0) n /= r;
+  return n == 1;
+}
+
+static uint32_t ld_f32(uint64_t n) { return (uint32_t)(n + (n >> 4) + 1); }
+
+static Schedule schedule_for(uint64_t n) {
+  Schedule sch;
+  std::memset(&sch, 0, sizeof(sch));
+  const std::vector<uint32_t> rad = stage_radices(n);
+  sch.N = (uint32_t)n;
+  sch.nst = (uint32_t)rad.size();
+  uint64_t Ns = 1;
+  for (size_t s = 0; s < rad.size(); ++s) {
+    StageDesc& d = sch.st[s];
+    d.R = rad[s];
+    d.Ns = (uint32_t)Ns;
+    d.NR = (uint32_t)(n / rad[s]);
+    d.tw_off = 0;
+    d.dNs = make_fastdiv((uint32_t)Ns);
+    d.dNR = make_fastdiv((uint32_t)(n / rad[s]));
+    Ns *= rad[s];
+  }
+  return sch;
+}
+
+static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
+  uint64_t r = 1;
+  b %= m;
+  while (e) {
+    if (e & 1) r = (unsigned __int128)r * b % m;
+    b = (unsigned __int128)b * b % m;
+    e >>= 1;
+  }
+  return r;
+}
+
+struct BatchPlan {
+  int device = 0;
+  int32_t direction = B2F_FORWARD, normalization = B2F_NORM_INVERSE;
+  uint64_t nlines = 0, extent = 0;  // extent: complex elements the buffers must hold
+  // device state
+  BatchLen* d_lens = nullptr;
+  BatchTask* d_tasks = nullptr;  // CTA tasks then cluster tasks
+  uint64_t* d_off = nullptr;
+  unsigned int* d_counters = nullptr;  // [0] CTA queue, [1] cluster queue
+  std::vector<void*> tables;
+  uint32_t n_cta = 0, n_cl = 0, n_big = 0;
+  unsigned grid_big = 0;
+  uint32_t buf_cta = 0, buf_cl = 0;
+  size_t smem_cta = 0, smem_cl = 0;
+  unsigned grid_cta = 0, grid_cl = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  // description
+  uint64_t lines_cta = 0, lines_cl = 0, distinct = 0, table_bytes = 0;
+  uint64_t elems_cta = 0, elems_cl = 0;
+  uint64_t kind_lines[5] = {0, 0, 0, 0, 0};
+  std::string diag;
+  ~BatchPlan() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (void* p : tables) cudaFree(p);
+    cudaFree(d_lens);
+    cudaFree(d_tasks);
+    cudaFree(d_off);
+    cudaFree(d_counters);
+    if (side) cudaStreamDestroy(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+constexpr int kClusterP = 8;
+constexpr int kClusterBig = 16;  // non-portable cluster size for the longest Bluestein lines
+constexpr unsigned kCtaThreads = 256;
+constexpr unsigned kClusterThreads = 512;
+
+struct LenInfo {
+  BatchLen d;
+  std::vector<cd> bhat;
+  std::vector<uint32_t> pin, pout;
+  double cost = 0;
+};
+
+// Chooses the execution of one distinct length.
+static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_t cta_cap,
+                     size_t cl_cap, LenInfo& li) {
+  BatchLen& d = li.d;
+  std::memset(&d, 0, sizeof(d));
+  d.N = (uint32_t)N;
+  const bool inv = direction == B2F_INVERSE;
+  float sc = 1.0f;
+  if ((normalization == B2F_NORM_INVERSE && inv) || (normalization == B2F_NORM_FORWARD && !inv))
+    sc = 1.0f / (float)N;
+  else if (normalization == B2F_NORM_ORTHOGONAL)
+    sc = 1.0f / sqrtf((float)N);
+  d.scale = sc;
+  d.dN = make_fastdiv((uint32_t)N);
+  const auto cta_bytes = [](uint64_t lbuf) { return 2 * (size_t)ld_f32(lbuf) * 8; };
+  // long smooth lines split over the cluster when a factor <= 8 allows it
+  uint32_t cl_split = 0;
+  if (is_smooth13(N) && cta_bytes(N) > cta_cap)
+    for (uint32_t P : {8u, 7u, 5u, 4u, 3u, 2u})
+      if (N % P == 0 && cta_bytes(N / P) <= cl_cap) {
+        cl_split = P;
+        break;
+      }
+  const bool smooth = is_smooth13(N) && (cta_bytes(N) <= cta_cap || cl_split);
+  if (smooth && cta_bytes(N) <= cta_cap) {
+    d.kind = BK_MIXED;
+    d.M = (uint32_t)N;
+    d.LD = ld_f32(N);
+    d.sch = schedule_for(N);
+  } else if (smooth) {
+    d.kind = BK_CL_MIXED;
+    d.M = (uint32_t)N;
+    d.P = cl_split;
+    d.L = (uint32_t)(N / cl_split);
+    d.LD = ld_f32(d.L);
+    d.sch = schedule_for(d.L);
+  } else if (is_prime_u64(N) && N >= 3 && is_smooth13(N - 1) && cta_bytes(N) <= cta_cap) {
+    d.kind = BK_RADER;
+    d.M = (uint32_t)(N - 1);
+    d.LD = ld_f32(N);
+    d.sch = schedule_for(N - 1);
+    d.dP1 = make_fastdiv((uint32_t)(N - 1));
+    const uint64_t g = primitive_root(N), ginv = mod_pow64(g, N - 2, N);
+    li.pin.resize(N - 1);
+    li.pout.resize(N - 1);
+    li.bhat.resize(N - 1);
+    uint64_t v = 1;
+    for (uint64_t q = 0; q + 1 < N; ++q) {
+      li.pin[q] = (uint32_t)v;
+      v = v * g % N;
+    }
+    v = 1;
+    for (uint64_t r = 0; r + 1 < N; ++r) {
+      li.pout[v - 1] = (uint32_t)r;
+      li.bhat[r] = root_fwd(v, N);
+      v = v * ginv % N;
+    }
+    host_fft_fwd(li.bhat);
+    for (auto& x : li.bhat) x /= (double)(N - 1);
+  } else {
+    uint64_t M = 2 * N - 1;
+    while (!smooth7(M)) ++M;
+    if (cta_bytes(M) <= cta_cap) {
+      d.kind = BK_BLUE;
+      d.M = (uint32_t)M;
+      d.LD = ld_f32(M);
+      d.sch = schedule_for(M);
+    } else {
+      // cluster Bluestein: convolution P*L >= 2N-1, L 7-smooth and fitting
+      uint32_t P = kClusterP;
+      uint64_t L = (2 * N - 1 + P - 1) / P;
+      while (!smooth7(L)) ++L;
+      if (cta_bytes(L) > cl_cap) {
+        P = kClusterBig;
+        L = (2 * N - 1 + P - 1) / P;
+        while (!smooth7(L)) ++L;
+        if (cta_bytes(L) > cl_cap) return false;
+      }
+      M = L * P;
+      d.kind = BK_CL_BLUE;
+      d.M = (uint32_t)M;
+      d.P = P;
+      d.L = (uint32_t)L;
+      d.LD = ld_f32(L);
+      d.sch = schedule_for(L);
+    }
+    d.dM = make_fastdiv((uint32_t)M);
+    d.dMN = make_fastdiv((uint32_t)(M - N));
+    li.bhat.assign(M, cd(0, 0));
+    for (uint64_t m = 0; m < N; ++m) {
+      const cd c = std::conj(chirp_fwd(m, N));
+      li.bhat[m] = c;
+      if (m) li.bhat[M - m] = c;
+    }
+    host_fft_fwd(li.bhat);
+    for (auto& x : li.bhat) x /= (double)M;
+  }
+  const double T = d.M;
+  li.cost = T * std::log2(std::max(2.0, T)) * (d.kind == BK_BLUE || d.kind == BK_CL_BLUE ? 3 : 1);
+  if (d.kind == BK_MIXED || d.kind == BK_RADER || d.kind == BK_BLUE) {
+    uint64_t G = std::max<uint64_t>(1, 4096 / d.M);
+    G = std::min<uint64_t>(G, kBatchMaxG);
+    while (G > 1 && G * cta_bytes(d.kind == BK_RADER ? N : d.M) > cta_cap) --G;
+    d.G = (uint32_t)G;
+  } else {
+    d.G = 1;
+  }
+  return true;
+}
+
+template <class K>
+static cudaError_t set_smem(K kernel, size_t smem) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets, uint64_t nlines,
+                               int32_t direction, int32_t normalization, int device,
+                               BatchPlan** out) {
+  *out = nullptr;
+  if (!lengths || !offsets || nlines == 0) return fail(B2F_ERR_INVALID_ARGUMENT, "empty batch");
+  if (direction != B2F_FORWARD && direction != B2F_INVERSE)
+    return fail(B2F_ERR_INVALID_ARGUMENT, "direction must be 0 or 1");
+  if (normalization < 0 || normalization > 3)
+    return fail(B2F_ERR_INVALID_ARGUMENT, "normalization must be 0..=3");
+  // lines must be non-empty and disjoint
+  std::vector<uint64_t> order(nlines);
+  for (uint64_t i = 0; i < nlines; ++i) {
+    order[i] = i;
+    if (lengths[i] == 0) return fail(B2F_ERR_ZERO_LENGTH, "ZeroLength: line " + std::to_string(i));
+    if (lengths[i] > 0xFFFFFFFFull) return fail(B2F_ERR_LENGTH_TOO_LARGE, "LengthTooLarge");
+  }
+  std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return offsets[a] < offsets[b]; });
+  uint64_t extent = 0;
+  for (uint64_t i = 0; i < nlines; ++i) {
+    const uint64_t l = order[i];
+    if (i && offsets[l] < offsets[order[i - 1]] + lengths[order[i - 1]])
+      return fail(B2F_ERR_INVALID_ARGUMENT, "batch lines overlap");
+    extent = std::max(extent, offsets[l] + lengths[l]);
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (device < 0) device = prev < 0 ? 0 : prev;
+  if (cudaSetDevice(device) != cudaSuccess) return fail(B2F_ERR_DEVICE, "cudaSetDevice failed");
+  std::unique_ptr<BatchPlan> bp(new BatchPlan());
+  bp->device = device;
+  bp->direction = direction;
+  bp->normalization = normalization;
+  bp->nlines = nlines;
+  bp->extent = extent;
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  const size_t static_smem = sizeof(BatchLen) + 2 * kBatchMaxG * 8 + 64;
+  const size_t cta_cap = 68 * 1024;  // line buffers of three CTAs per SM
+  const size_t cl_cap = (size_t)smem_optin - static_smem - 1024;
+  // distinct lengths
+  std::map<uint64_t, std::vector<uint64_t>> by_len;
+  for (uint64_t i = 0; i < nlines; ++i) by_len[lengths[i]].push_back(i);
+  std::vector<uint64_t> lens_list;
+  for (auto& kv : by_len) lens_list.push_back(kv.first);
+  std::vector<LenInfo> infos(lens_list.size());
+  std::vector<int> ok(lens_list.size(), 0);
+  {
+    const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned w = 0; w < nth; ++w)
+      th.emplace_back([&, w] {
+        for (size_t i = w; i < lens_list.size(); i += nth)
+          ok[i] = classify(lens_list[i], direction, normalization, cta_cap, cl_cap, infos[i]);
+      });
+    for (auto& t : th) t.join();
+  }
+  for (size_t i = 0; i < lens_list.size(); ++i)
+    if (!ok[i]) {
+      if (prev >= 0) cudaSetDevice(prev);
+      return fail(B2F_ERR_UNSUPPORTED_LENGTH,
+                  "UnsupportedLength { len: " + std::to_string(lens_list[i]) + " } in a batch");
+    }
+  bp->distinct = lens_list.size();
+  // tables
+  auto upload = [&](const void* src, size_t bytes, void** dst) -> bool {
+    if (bytes == 0) {
+      *dst = nullptr;
+      return true;
+    }
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
+    bp->tables.push_back(*dst);
+    bp->table_bytes += bytes;
+    return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  for (auto& li : infos) {
+    if (!li.bhat.empty()) {
+      std::vector<float> f(li.bhat.size() * 2);
+      for (size_t i = 0; i < li.bhat.size(); ++i) {
+        f[2 * i] = (float)li.bhat[i].real();
+        f[2 * i + 1] = (float)li.bhat[i].imag();
+      }
+      void* p;
+      if (!upload(f.data(), f.size() * 4, &p)) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch table allocation failed");
+      li.d.bhat = (const c32*)p;
+    }
+    if (!li.pin.empty()) {
+      void *a, *b;
+      if (!upload(li.pin.data(), li.pin.size() * 4, &a) || !upload(li.pout.data(), li.pout.size() * 4, &b))
+        return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch table allocation failed");
+      li.d.perm_in = (const uint32_t*)a;
+      li.d.perm_out = (const uint32_t*)b;
+    }
+  }
+  // tasks: CTA tasks (groups of G lines of one length), cluster tasks (one line each)
+  std::vector<uint64_t> sorted_off;
+  std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks;
+  std::vector<double> cta_cost, cl_cost, big_cost;
+  std::vector<uint32_t> order_len(lens_list.size());
+  for (size_t i = 0; i < lens_list.size(); ++i) order_len[i] = (uint32_t)i;
+  // lines sorted by length index; tasks reference contiguous runs
+  for (size_t li = 0; li < lens_list.size(); ++li) {
+    const auto& lines = by_len[lens_list[li]];
+    const BatchLen& d = infos[li].d;
+    bp->kind_lines[d.kind] += lines.size();
+    const bool cl = d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE;
+    for (size_t s = 0; s < lines.size(); s += (cl ? 1 : d.G)) {
+      BatchTask t;
+      t.len = (uint32_t)li;
+      t.first = (uint32_t)sorted_off.size();
+      t.count = (uint32_t)std::min<size_t>(cl ? 1 : d.G, lines.size() - s);
+      t.pad = 0;
+      for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[lines[s + c]]);
+      if (cl && d.P == kClusterBig) {
+        big_tasks.push_back(t);
+        big_cost.push_back(infos[li].cost);
+        bp->lines_cl += 1;
+        bp->elems_cl += lens_list[li];
+      } else if (cl) {
+        cl_tasks.push_back(t);
+        cl_cost.push_back(infos[li].cost);
+        bp->lines_cl += 1;
+        bp->elems_cl += lens_list[li];
+      } else {
+        cta_tasks.push_back(t);
+        cta_cost.push_back(infos[li].cost * t.count);
+        bp->lines_cta += t.count;
+        bp->elems_cta += lens_list[li] * t.count;
+      }
+    }
+  }
+  // longest first (the queue hands them out in order)
+  auto sort_by_cost = [](std::vector<BatchTask>& t, std::vector<double>& c) {
+    std::vector<size_t> idx(t.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return c[a] > c[b]; });
+    std::vector<BatchTask> out(t.size());
+    for (size_t i = 0; i < idx.size(); ++i) out[i] = t[idx[i]];
+    t.swap(out);
+  };
+  sort_by_cost(cta_tasks, cta_cost);
+  sort_by_cost(cl_tasks, cl_cost);
+  sort_by_cost(big_tasks, big_cost);
+  bp->n_cta = (uint32_t)cta_tasks.size();
+  bp->n_cl = (uint32_t)cl_tasks.size();
+  bp->n_big = (uint32_t)big_tasks.size();
+  // shared memory of each kernel: the largest task it runs
+  uint32_t buf_cta = 1, buf_cl = 1;
+  for (auto& li : infos) {
+    const BatchLen& d = li.d;
+    if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) buf_cl = std::max(buf_cl, d.LD);
+    else buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
+  }
+  bp->buf_cta = buf_cta;
+  bp->buf_cl = buf_cl;
+  bp->smem_cta = 2 * (size_t)buf_cta * 8 + 2 * kBatchMaxG * 8;
+  bp->smem_cl = 2 * (size_t)buf_cl * 8;
+  // device arrays
+  std::vector<BatchLen> dl(infos.size());
+  for (size_t i = 0; i < infos.size(); ++i) dl[i] = infos[i].d;
+  std::vector<BatchTask> all = cta_tasks;
+  all.insert(all.end(), cl_tasks.begin(), cl_tasks.end());
+  all.insert(all.end(), big_tasks.begin(), big_tasks.end());
+  bool okc = cudaMalloc(&bp->d_lens, dl.size() * sizeof(BatchLen)) == cudaSuccess &&
+             cudaMalloc(&bp->d_tasks, std::max<size_t>(1, all.size()) * sizeof(BatchTask)) == cudaSuccess &&
+             cudaMalloc(&bp->d_off, sorted_off.size() * 8) == cudaSuccess &&
+             cudaMalloc(&bp->d_counters, 4 * sizeof(unsigned int)) == cudaSuccess;
+  if (!okc) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
+  cudaMemcpy(bp->d_lens, dl.data(), dl.size() * sizeof(BatchLen), cudaMemcpyHostToDevice);
+  if (!all.empty()) cudaMemcpy(bp->d_tasks, all.data(), all.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
+  cudaMemcpy(bp->d_off, sorted_off.data(), sorted_off.size() * 8, cudaMemcpyHostToDevice);
+  // launch shapes
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (bp->n_cta) {
+    if (set_smem(k_batch_cta, bp->smem_cta) != cudaSuccess)
+      return fail(B2F_ERR_DEVICE, "batch CTA kernel shared memory");
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cta, kCtaThreads, bp->smem_cta);
+    per_sm = std::max(per_sm, 1);
+    bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, bp->n_cta);
+  }
+  if (bp->n_cl) {
+    if (set_smem(k_batch_cluster<kClusterP>, bp->smem_cl) != cudaSuccess)
+      return fail(B2F_ERR_DEVICE, "batch cluster kernel shared memory");
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterP;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(kClusterP * 64, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = bp->smem_cl;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_batch_cluster<kClusterP>, &cfg) != cudaSuccess ||
+        nclusters <= 0) {
+      cudaGetLastError();
+      return fail(B2F_ERR_DEVICE, "no thread-block cluster of 8 CTAs fits this device");
+    }
+    bp->grid_cl = (unsigned)(kClusterP * std::min<uint64_t>((uint64_t)nclusters, bp->n_cl));
+  }
+  if (bp->n_big) {
+    if (set_smem(k_batch_cluster<kClusterBig>, bp->smem_cl) != cudaSuccess ||
+        cudaFuncSetAttribute(k_batch_cluster<kClusterBig>,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+      return fail(B2F_ERR_DEVICE, "batch 16-CTA cluster kernel attributes");
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterBig;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(kClusterBig * 16, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = bp->smem_cl;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_batch_cluster<kClusterBig>, &cfg) != cudaSuccess ||
+        nclusters <= 0) {
+      cudaGetLastError();
+      return fail(B2F_ERR_UNSUPPORTED_LENGTH,
+                  "UnsupportedLength: a Bluestein line needs a 16-CTA cluster, which this device cannot schedule");
+    }
+    bp->grid_big = (unsigned)(kClusterBig * std::min<uint64_t>((uint64_t)nclusters, bp->n_big));
+  }
+  if (cudaStreamCreateWithFlags(&bp->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&bp->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&bp->join, cudaEventDisableTiming) != cudaSuccess)
+    return fail(B2F_ERR_DEVICE, "batch stream creation failed");
+  std::ostringstream os;
+  os << "{\"lines\":" << nlines << ",\"distinct_lengths\":" << bp->distinct
+     << ",\"cta_lines\":" << bp->lines_cta << ",\"cluster_lines\":" << bp->lines_cl
+     << ",\"cta_elements\":" << bp->elems_cta << ",\"cluster_elements\":" << bp->elems_cl
+     << ",\"cta_tasks\":" << bp->n_cta << ",\"cluster_tasks\":" << bp->n_cl
+     << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
+     << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
+     << ",\"cluster_bluestein\":" << bp->kind_lines[4] << "}"
+     << ",\"cta_grid\":" << bp->grid_cta << ",\"cta_threads\":" << kCtaThreads
+     << ",\"cta_smem\":" << bp->smem_cta << ",\"cluster_grid\":" << bp->grid_cl
+     << ",\"cluster_size\":" << kClusterP << ",\"cluster16_tasks\":" << bp->n_big
+     << ",\"cluster16_grid\":" << bp->grid_big << ",\"cluster_threads\":" << kClusterThreads
+     << ",\"cluster_smem\":" << bp->smem_cl << ",\"table_bytes\":" << bp->table_bytes
+     << ",\"required_buffer_size_bytes\":" << extent * 8 << "}";
+  bp->diag = os.str();
+  if (prev >= 0) cudaSetDevice(prev);
+  *out = bp.release();
+  return B2F_OK;
+}
+
+static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in, void* out,
+                            uint32_t parts = 3, bool sequential = false) {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != bp.device) cudaSetDevice(bp.device);
+  cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, 4 * sizeof(unsigned int), st);
+  BatchParams p{};
+  p.in = (const c32*)in;
+  p.out = (c32*)out;
+  p.lens = bp.d_lens;
+  p.line_off = bp.d_off;
+  p.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
+  const bool run_cl = (bp.n_cl || bp.n_big) && (parts & 2);
+  const bool run_cta = bp.n_cta && (parts & 1);
+  cudaStream_t cl_stream = sequential ? st : bp.side;
+  if (e == cudaSuccess && run_cl) {
+    // long lines on a forked stream, concurrently with the CTA queue
+    if (!sequential) {
+      e = cudaEventRecord(bp.fork, st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(bp.side, bp.fork, 0);
+    }
+    BatchParams pc = p;
+    pc.tasks = bp.d_tasks + bp.n_cta;
+    pc.ntasks = bp.n_cl;
+    pc.counter = bp.d_counters + 1;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterP;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(bp.grid_cl, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = bp.smem_cl;
+    cfg.stream = cl_stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (e == cudaSuccess && bp.n_cl) e = cudaLaunchKernelEx(&cfg, k_batch_cluster<kClusterP>, pc, bp.buf_cl);
+    if (e == cudaSuccess && bp.n_big) {
+      BatchParams pb = p;
+      pb.tasks = bp.d_tasks + bp.n_cta + bp.n_cl;
+      pb.ntasks = bp.n_big;
+      pb.counter = bp.d_counters + 2;
+      attr[0].val.clusterDim.x = kClusterBig;
+      cfg.gridDim = dim3(bp.grid_big, 1, 1);
+      e = cudaLaunchKernelEx(&cfg, k_batch_cluster<kClusterBig>, pb, bp.buf_cl);
+    }
+  }
+  if (e == cudaSuccess && run_cta) {
+    BatchParams pt = p;
+    pt.tasks = bp.d_tasks;
+    pt.ntasks = bp.n_cta;
+    pt.counter = bp.d_counters;
+    k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && run_cl && !sequential) {
+    e = cudaEventRecord(bp.join, bp.side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bp.join, 0);
+  }
+  if (prev >= 0 && prev != bp.device) cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(B2F_ERR_DEVICE, std::string("batch launch failed: ") + cudaGetErrorString(e));
+  return B2F_OK;
+}
+
+}  // namespace b2f
+
+using namespace b2f;
+
+struct b2f_batch {
+  BatchPlan* plan;
+};
+
+extern "C" {
+
+b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
+                         uint64_t nlines, int32_t direction, int32_t normalization,
+                         int32_t device) {
+  if (!out) return fail(B2F_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  BatchPlan* p = nullptr;
+  b2f_status st = create_batch(lengths, offsets, nlines, direction, normalization, device, &p);
+  if (st) return st;
+  *out = new b2f_batch{p};
+  return B2F_OK;
+}
+
+void b2f_batch_free(b2f_batch* b) {
+  if (!b) return;
+  delete b->plan;
+  delete b;
+}
+
+uint64_t b2f_batch_required_buffer_size_bytes(const b2f_batch* b) {
+  return b ? b->plan->extent * 8 : 0;
+}
+
+b2f_status b2f_batch_execute(const b2f_batch* b, void* stream, const void* in, uint64_t in_bytes,
+                             void* out, uint64_t out_bytes) {
+  if (!b || !in || !out) return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
+  const uint64_t need = b->plan->extent * 8;
+  if (in_bytes < need || out_bytes < need)
+    return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall { required: " + std::to_string(need) + " }");
+  return run_batch(*b->plan, (cudaStream_t)stream, in, out);
+}
+
+b2f_status b2f_batch_execute_parts(const b2f_batch* b, void* stream, const void* in,
+                                   uint64_t in_bytes, void* out, uint64_t out_bytes,
+                                   uint32_t parts, int32_t sequential) {
+  if (!b || !in || !out) return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
+  const uint64_t need = b->plan->extent * 8;
+  if (in_bytes < need || out_bytes < need)
+    return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall { required: " + std::to_string(need) + " }");
+  return run_batch(*b->plan, (cudaStream_t)stream, in, out, parts, sequential != 0);
+}
+
+b2f_status b2f_batch_diagnostics_json(const b2f_batch* b, char* buf, uint64_t* len) {
+  if (!b || !len) return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
+  const std::string& j = b->plan->diag;
+  const uint64_t cap = *len;
+  *len = j.size();
+  if (buf && cap > 0) {
+    const uint64_t n = std::min<uint64_t>(cap - 1, j.size());
+    std::memcpy(buf, j.data(), n);
+    buf[n] = 0;
+    if (n < j.size()) return fail(B2F_ERR_BUFFER_TOO_SMALL, "diagnostics buffer too small");
+  }
+  return B2F_OK;
+}
+
+}  // extern "C"

@@ -45,6 +45,36 @@ struct PadOf {
   static constexpr int value = (sizeof(cpx<S>) == 8) ? 4 : 3;
 };
 
+// Stage twiddles W_M^{q k}, q = 1..R-1, computed in-kernel: W^k and W^{4k}
+// from the octant-reduced sincospi, the others as products of at most three
+// of those (each product adds about one rounding), so no table is read.
+template <class S, int R>
+FFT_D void apply_stage_twiddles(cpx<S>* v, uint32_t k, uint32_t M) {
+  if constexpr (R <= 3) {
+    const cpx<S> w1 = twiddle<S>(k, M);
+    v[1] = cmul(v[1], w1);
+    if constexpr (R == 3) v[2] = cmul(v[2], twiddle<S>(2 * k, M));
+  } else {
+    cpx<S> w[R];
+    w[1] = twiddle<S>(k, M);
+    w[2] = cmul(w[1], w[1]);
+#pragma unroll
+    for (int q = 3; q < R && q < 4; ++q) w[q] = cmul(w[q - 1], w[1]);
+    if constexpr (R > 4) {
+      w[4] = twiddle<S>(4 * k, M);
+#pragma unroll
+      for (int q = 5; q < R && q < 8; ++q) w[q] = cmul(w[4], w[q - 4]);
+    }
+    if constexpr (R > 8) {
+      w[8] = cmul(w[4], w[4]);
+#pragma unroll
+      for (int q = 9; q < R; ++q) w[q] = cmul(w[8], w[q - 8]);
+    }
+#pragma unroll
+    for (int q = 1; q < R; ++q) v[q] = cmul(v[q], w[q]);
+  }
+}
+
 // One radix-R stage over the G lines of the CTA, src -> dst.  Butterfly b
 // maps to line l = b / (N/R) and position j = b % (N/R); k = j % Ns selects
 // the twiddles W_{Ns R}^{q k}.
@@ -69,8 +99,7 @@ FFT_D void fft_stage(const cpx<S>* __restrict__ src, cpx<S>* __restrict__ dst,
 #pragma unroll
         for (int q = 1; q < R; ++q) v[q] = cmul(v[q], t[q - 1]);
       } else {
-#pragma unroll
-        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle<S>(q * k, M));
+        apply_stage_twiddles<S, R>(v, k, M);
       }
     }
     dft<S, R>(v);

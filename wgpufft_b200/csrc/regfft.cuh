@@ -34,8 +34,7 @@ FFT_D void reg_stage_compute(C<S> (&v)[E], uint32_t t, uint32_t TL, uint32_t Ns,
 #pragma unroll
         for (int q = 1; q < R; ++q) v[u * R + q] = cmul(v[u * R + q], tr[q - 1]);
       } else {
-#pragma unroll
-        for (int q = 1; q < R; ++q) v[u * R + q] = cmul(v[u * R + q], twiddle<S>(q * k, M));
+        apply_stage_twiddles<S, R>(v + u * R, k, M);
       }
     }
   }

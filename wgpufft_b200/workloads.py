@@ -1,0 +1,79 @@
+"""Seeded synthetic workloads of the benchmark configurations (no datasets:
+every input is generated from a fixed seed with the stated shape and value
+distribution)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _is_smooth13(n: int) -> bool:
+    for p in (2, 3, 5, 7, 11, 13):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def _is_prime(n: int) -> bool:
+    if n < 2:
+        return False
+    if n % 2 == 0:
+        return n == 2
+    d = 3
+    while d * d <= n:
+        if n % d == 0:
+            return False
+        d += 2
+    return True
+
+
+def _nearest(n: int, pred, lo: int, hi: int) -> int:
+    for d in range(0, hi):
+        for c in (n - d, n + d):
+            if lo <= c <= hi and pred(c):
+                return c
+    raise ValueError("no candidate")
+
+
+def mixed_lengths(count: int = 20000, seed: int = 5, lo: int = 16, hi: int = 65536):
+    """Line lengths log-uniform in [lo, hi]; by a seeded draw 70% snapped to
+    the nearest 13-smooth length, 15% to the nearest prime and 15% to the
+    nearest composite with a prime factor above 13."""
+    rng = np.random.default_rng(seed)
+    raw = np.exp(rng.uniform(math.log(lo), math.log(hi), count))
+    cls = rng.uniform(0.0, 1.0, count)
+    out = []
+    for r, c in zip(raw, cls):
+        n = int(round(r))
+        if c < 0.70:
+            out.append(_nearest(n, _is_smooth13, lo, hi))
+        elif c < 0.85:
+            out.append(_nearest(n, _is_prime, lo, hi))
+        else:
+            out.append(_nearest(n, lambda m: m > 3 and not _is_prime(m) and not _is_smooth13(m),
+                                lo, hi))
+    return np.asarray(out, dtype=np.int64)
+
+
+def packed_offsets(lengths) -> np.ndarray:
+    """Lines stored back to back: offset of each line in complex elements."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    off = np.zeros(len(lengths), dtype=np.int64)
+    if len(lengths) > 1:
+        off[1:] = np.cumsum(lengths[:-1])
+    return off
+
+
+def normal_complex(n: int, seed: int) -> np.ndarray:
+    """iid N(0,1) real and imaginary parts as complex64."""
+    rng = np.random.default_rng(seed)
+    x = np.empty(n, dtype=np.complex64)
+    x.real = rng.standard_normal(n, dtype=np.float32)
+    x.imag = rng.standard_normal(n, dtype=np.float32)
+    return x
+
+
+def fft_flops(n: int) -> float:
+    """The 5 N log2 N convention for one complex transform of length N."""
+    return 5.0 * n * math.log2(n) if n > 1 else 0.0
