@@ -44,6 +44,30 @@ static Schedule schedule_for(uint64_t n) {
   return sch;
 }
 
+// Appends the stage twiddles of sch (rows k*(R-1) + q-1 per stage) to tw
+// once per FFT length and points the stages at them.
+static void attach_stage_table(Schedule& sch, std::vector<cd>& tw,
+                               std::map<uint32_t, uint32_t>& cache) {
+  auto it = cache.find(sch.N);
+  uint32_t base;
+  if (it != cache.end()) {
+    base = it->second;
+  } else {
+    base = (uint32_t)tw.size();
+    cache[sch.N] = base;
+    for (uint32_t s = 0; s < sch.nst; ++s) {
+      const uint32_t R = sch.st[s].R, Ns = sch.st[s].Ns;
+      for (uint64_t k = 0; k < Ns; ++k)
+        for (uint32_t q = 1; q < R; ++q) tw.push_back(root_fwd(q * k, (uint64_t)Ns * R));
+    }
+  }
+  uint32_t off = base;
+  for (uint32_t s = 0; s < sch.nst; ++s) {
+    sch.st[s].tw_off = off;
+    off += sch.st[s].Ns * (sch.st[s].R - 1);
+  }
+}
+
 static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
   uint64_t r = 1;
   b %= m;
@@ -75,7 +99,12 @@ struct BatchPlan {
   // description
   uint64_t lines_cta = 0, lines_cl = 0, distinct = 0, table_bytes = 0;
   uint64_t elems_cta = 0, elems_cl = 0;
-  uint64_t kind_lines[5] = {0, 0, 0, 0, 0};
+  uint64_t slot_elems = 0;  // BK_LONG scratch slot per CTA
+  c32* d_scratch = nullptr;
+  c32* d_tw = nullptr;
+  uint64_t tw_bytes = 0;
+  uint64_t scratch_bytes = 0;
+  uint64_t kind_lines[6] = {0, 0, 0, 0, 0, 0};
   std::string diag;
   ~BatchPlan() {
     int prev = -1;
@@ -86,6 +115,8 @@ struct BatchPlan {
     cudaFree(d_tasks);
     cudaFree(d_off);
     cudaFree(d_counters);
+    cudaFree(d_scratch);
+    cudaFree(d_tw);
     if (side) cudaStreamDestroy(side);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
@@ -120,27 +151,36 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   d.scale = sc;
   d.dN = make_fastdiv((uint32_t)N);
   const auto cta_bytes = [](uint64_t lbuf) { return 2 * (size_t)ld_f32(lbuf) * 8; };
-  // long smooth lines split over the cluster when a factor <= 8 allows it
-  uint32_t cl_split = 0;
-  if (is_smooth13(N) && cta_bytes(N) > cta_cap)
-    for (uint32_t P : {8u, 7u, 5u, 4u, 3u, 2u})
-      if (N % P == 0 && cta_bytes(N / P) <= cl_cap) {
-        cl_split = P;
-        break;
+  // long smooth lines: two passes N = N1 * N2 inside one CTA, both <= 256,
+  // as balanced as the divisors allow
+  uint64_t n1 = 0;
+  if (is_smooth13(N) && cta_bytes(N) > cta_cap) {
+    double best = 1e300;
+    for (uint64_t a = 2; a <= 256; ++a) {
+      if (N % a || N / a > 256) continue;
+      const double bal = std::fabs(std::log((double)a) - std::log((double)(N / a)));
+      if (bal < best) {
+        best = bal;
+        n1 = a;
       }
-  const bool smooth = is_smooth13(N) && (cta_bytes(N) <= cta_cap || cl_split);
+    }
+  }
+  const bool smooth = is_smooth13(N) && (cta_bytes(N) <= cta_cap || n1);
   if (smooth && cta_bytes(N) <= cta_cap) {
     d.kind = BK_MIXED;
     d.M = (uint32_t)N;
     d.LD = ld_f32(N);
     d.sch = schedule_for(N);
   } else if (smooth) {
-    d.kind = BK_CL_MIXED;
+    d.kind = BK_LONG;
     d.M = (uint32_t)N;
-    d.P = cl_split;
-    d.L = (uint32_t)(N / cl_split);
-    d.LD = ld_f32(d.L);
-    d.sch = schedule_for(d.L);
+    d.N1 = (uint32_t)n1;
+    d.N2 = (uint32_t)(N / n1);
+    d.LD1 = ld_f32(d.N1);
+    d.LD2 = ld_f32(d.N2);
+    d.LD = std::max(d.LD1, d.LD2);
+    d.sch = schedule_for(d.N1);
+    d.sch2 = schedule_for(d.N2);
   } else if (is_prime_u64(N) && N >= 3 && is_smooth13(N - 1) && cta_bytes(N) <= cta_cap) {
     d.kind = BK_RADER;
     d.M = (uint32_t)(N - 1);
@@ -204,7 +244,9 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   }
   const double T = d.M;
   li.cost = T * std::log2(std::max(2.0, T)) * (d.kind == BK_BLUE || d.kind == BK_CL_BLUE ? 3 : 1);
-  if (d.kind == BK_MIXED || d.kind == BK_RADER || d.kind == BK_BLUE) {
+  if (d.kind == BK_LONG) {
+    d.G = 1;
+  } else if (d.kind == BK_MIXED || d.kind == BK_RADER || d.kind == BK_BLUE) {
     uint64_t G = std::max<uint64_t>(1, 4096 / d.M);
     G = std::min<uint64_t>(G, kBatchMaxG);
     while (G > 1 && G * cta_bytes(d.kind == BK_RADER ? N : d.M) > cta_cap) --G;
@@ -215,9 +257,10 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   return true;
 }
 
+// Opts the kernel in to `smem` bytes of dynamic shared memory (needed as
+// soon as static plus dynamic shared memory exceeds 48 KB).
 template <class K>
 static cudaError_t set_smem(K kernel, size_t smem) {
-  if (smem <= 48 * 1024) return cudaSuccess;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
@@ -258,7 +301,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   int smem_optin = 0;
   cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   const size_t static_smem = sizeof(BatchLen) + 2 * kBatchMaxG * 8 + 64;
-  const size_t cta_cap = 68 * 1024;  // line buffers of three CTAs per SM
+  const size_t cta_cap = 44 * 1024;  // line buffers of four CTAs per SM
   const size_t cl_cap = (size_t)smem_optin - static_smem - 1024;
   // distinct lengths
   std::map<uint64_t, std::vector<uint64_t>> by_len;
@@ -284,6 +327,40 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
                   "UnsupportedLength { len: " + std::to_string(lens_list[i]) + " } in a batch");
     }
   bp->distinct = lens_list.size();
+  // twiddle tables shared by every length of the batch
+  {
+    std::vector<cd> tw;
+    std::map<uint32_t, uint32_t> cache;
+    for (auto& li : infos) {
+      BatchLen& d = li.d;
+      attach_stage_table(d.sch, tw, cache);
+      if (d.kind == BK_LONG) {
+        attach_stage_table(d.sch2, tw, cache);
+        d.ta = (uint32_t)tw.size();
+        for (uint32_t a = 0; a < d.N1; ++a) tw.push_back(root_fwd((uint64_t)a * d.N2, d.N));
+        d.tb = (uint32_t)tw.size();
+        for (uint32_t c = 0; c < d.N2; ++c) tw.push_back(root_fwd(c, d.N));
+        d.dB = make_fastdiv(d.N2);
+      } else if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) {
+        d.ta = (uint32_t)tw.size();
+        for (uint32_t a = 0; a < d.P; ++a) tw.push_back(root_fwd((uint64_t)a * d.L, d.M));
+        d.tb = (uint32_t)tw.size();
+        for (uint32_t c = 0; c < d.L; ++c) tw.push_back(root_fwd(c, d.M));
+        d.dB = make_fastdiv(d.L);
+      }
+    }
+    std::vector<float> f(std::max<size_t>(2, tw.size() * 2));
+    for (size_t i = 0; i < tw.size(); ++i) {
+      f[2 * i] = (float)tw[i].real();
+      f[2 * i + 1] = (float)tw[i].imag();
+    }
+    if (cudaMalloc(&bp->d_tw, f.size() * 4) != cudaSuccess ||
+        cudaMemcpy(bp->d_tw, f.data(), f.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      if (prev >= 0) cudaSetDevice(prev);
+      return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch twiddle table allocation failed");
+    }
+    bp->tw_bytes = f.size() * 4;
+  }
   // tables
   auto upload = [&](const void* src, size_t bytes, void** dst) -> bool {
     if (bytes == 0) {
@@ -371,7 +448,9 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   for (auto& li : infos) {
     const BatchLen& d = li.d;
     if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) buf_cl = std::max(buf_cl, d.LD);
+    else if (d.kind == BK_LONG) buf_cta = std::max<uint32_t>(buf_cta, kLongG * d.LD);
     else buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
+    if (d.kind == BK_LONG) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, d.N);
   }
   bp->buf_cta = buf_cta;
   bp->buf_cl = buf_cl;
@@ -401,6 +480,11 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cta, kCtaThreads, bp->smem_cta);
     per_sm = std::max(per_sm, 1);
     bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, bp->n_cta);
+    if (bp->slot_elems) {
+      bp->scratch_bytes = (uint64_t)bp->grid_cta * bp->slot_elems * 8;
+      if (cudaMalloc(&bp->d_scratch, bp->scratch_bytes) != cudaSuccess)
+        return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch scratch allocation failed");
+    }
   }
   if (bp->n_cl) {
     if (set_smem(k_batch_cluster<kClusterP>, bp->smem_cl) != cudaSuccess)
@@ -460,7 +544,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
      << ",\"cta_tasks\":" << bp->n_cta << ",\"cluster_tasks\":" << bp->n_cl
      << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
      << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
-     << ",\"cluster_bluestein\":" << bp->kind_lines[4] << "}"
+     << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5] << "}"
+     << ",\"scratch_bytes\":" << bp->scratch_bytes << ",\"twiddle_table_bytes\":" << bp->tw_bytes
      << ",\"cta_grid\":" << bp->grid_cta << ",\"cta_threads\":" << kCtaThreads
      << ",\"cta_smem\":" << bp->smem_cta << ",\"cluster_grid\":" << bp->grid_cl
      << ",\"cluster_size\":" << kClusterP << ",\"cluster16_tasks\":" << bp->n_big
@@ -485,6 +570,9 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
   p.lens = bp.d_lens;
   p.line_off = bp.d_off;
   p.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
+  p.scratch = bp.d_scratch;
+  p.tw = bp.d_tw;
+  p.slot_elems = bp.slot_elems;
   const bool run_cl = (bp.n_cl || bp.n_big) && (parts & 2);
   const bool run_cta = bp.n_cta && (parts & 1);
   cudaStream_t cl_stream = sequential ? st : bp.side;

@@ -31,6 +31,7 @@ enum BatchKind : uint32_t {
   BK_BLUE = 2,      // one CTA, Bluestein
   BK_CL_MIXED = 3,  // cluster, mixed radix (T = N)
   BK_CL_BLUE = 4,   // cluster, Bluestein (T = convolution length)
+  BK_LONG = 5,      // one CTA, two passes N = N1*N2 through an L2-resident scratch slot
 };
 
 struct BatchLen {
@@ -46,7 +47,14 @@ struct BatchLen {
   const uint32_t* perm_in;
   const uint32_t* perm_out;
   FastDiv dN, dM, dMN, dP1;
-  Schedule sch;   // schedule of the per-CTA FFT length (N, p-1, M or L)
+  uint32_t N1, N2, LD1, LD2;  // BK_LONG: N = N1 * N2, pitches of the two passes
+  // two-level tables of the inter-pass twiddle W_T^j, j = a*B + b (offsets
+  // into BatchParams::tw): ta[a] = W_T^{a B}, tb[b] = W_T^b.
+  //   BK_LONG: T = N, B = N2 (a < N1);  cluster kinds: T = M, B = L (a < P).
+  uint32_t ta, tb;
+  FastDiv dB;
+  Schedule sch;   // schedule of the per-CTA FFT length (N, p-1, M, L or N1)
+  Schedule sch2;  // BK_LONG: schedule of N2
 };
 
 struct BatchTask {
@@ -59,6 +67,9 @@ struct BatchTask {
 struct BatchParams {
   const c32* in;
   c32* out;
+  c32* scratch;          // BK_LONG: one slot of slot_elems per CTA
+  uint64_t slot_elems;
+  const c32* tw;         // stage and inter-pass twiddle tables (FP64-built, rounded once)
   const BatchLen* lens;
   const BatchTask* tasks;
   const uint64_t* line_off;  // complex offset of each line (sorted order)
@@ -69,12 +80,28 @@ struct BatchParams {
 
 constexpr int kBatchMaxG = 256;
 
+// Asynchronous 8-byte global -> shared copy (sm_80+ LDGSTS): every thread
+// keeps all of its loads in flight instead of waiting on each one.
+FFT_D void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+FFT_D void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 template <class T>
 FFT_D void copy_words(T* dst, const T* src, uint32_t tid, uint32_t nthreads) {
   static_assert(sizeof(T) % 4 == 0, "word copy");
   const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
   uint32_t* d = reinterpret_cast<uint32_t*>(dst);
   for (uint32_t i = tid; i < sizeof(T) / 4; i += nthreads) d[i] = s[i];
+}
+
+// W_T^j from the two-level table: j = a*B + b.
+FFT_D c32 tw2(const BatchParams& bp, const BatchLen& L, uint32_t j, uint32_t B) {
+  const uint32_t a = fdiv(j, L.dB), b = j - a * B;
+  return cmul(bp.tw[L.ta + a], bp.tw[L.tb + b]);
 }
 
 // --------------------------------------------------------------- CTA tasks
@@ -85,12 +112,18 @@ FFT_D void batch_mixed(const BatchParams& bp, const BatchLen& L, const int64_t* 
   const bool inv = bp.inverse;
   for (uint32_t e = tid; e < cnt * N; e += T) {
     const uint32_t c = fdiv(e, L.dN), n = e - c * N;
-    c32 v = bp.in[base[c] + n];
-    if (inv) v.im = -v.im;
-    A[c * LD + pidx<PAD>(n)] = v;
+    cp_async8(&A[c * LD + pidx<PAD>(n)], &bp.in[base[c] + n]);
+  }
+  cp_async_wait_all();
+  if (inv) {
+    for (uint32_t e = tid; e < cnt * N; e += T) {
+      const uint32_t c = fdiv(e, L.dN), n = e - c * N;
+      c32& v = A[c * LD + pidx<PAD>(n)];
+      v.im = -v.im;
+    }
   }
   __syncthreads();
-  const c32* r = fft_lines_smem<float>(A, B, L.sch, cnt, LD, tid, T, nullptr);
+  const c32* r = fft_lines_smem<float>(A, B, L.sch, cnt, LD, tid, T, bp.tw);
   const float sc = L.scale;
   for (uint32_t e = tid; e < cnt * N; e += T) {
     const uint32_t c = fdiv(e, L.dN), n = e - c * N;
@@ -119,7 +152,7 @@ FFT_D void batch_rader(const BatchParams& bp, const BatchLen& L, const int64_t* 
     B[l * LD + pidx<PAD>(q)] = A[l * LD + pidx<PAD>(L.perm_in[q])];
   }
   __syncthreads();
-  c32* r1 = fft_lines_smem<float>(B, A, L.sch, cnt, LD, tid, T, nullptr);
+  c32* r1 = fft_lines_smem<float>(B, A, L.sch, cnt, LD, tid, T, bp.tw);
   c32* o1 = (r1 == A) ? B : A;
   if (tid < cnt) X0s[tid] = x0s[tid] + r1[tid * LD];
   __syncthreads();
@@ -130,7 +163,7 @@ FFT_D void batch_rader(const BatchParams& bp, const BatchLen& L, const int64_t* 
     r1[l * LD + pidx<PAD>(m)] = v;
   }
   __syncthreads();
-  const c32* r2 = fft_lines_smem<float>(r1, o1, L.sch, cnt, LD, tid, T, nullptr);
+  const c32* r2 = fft_lines_smem<float>(r1, o1, L.sch, cnt, LD, tid, T, bp.tw);
   const float sc = L.scale;
   for (uint32_t e = tid; e < cnt * P; e += T) {
     const uint32_t c = fdiv(e, L.dN), n = e - c * P;
@@ -164,7 +197,7 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
     A[c * LD + pidx<PAD>(m)] = v;
   }
   __syncthreads();
-  c32* r1 = fft_lines_smem<float>(A, B, L.sch, cnt, LD, tid, T, nullptr);
+  c32* r1 = fft_lines_smem<float>(A, B, L.sch, cnt, LD, tid, T, bp.tw);
   c32* o1 = (r1 == A) ? B : A;
   for (uint32_t e = tid; e < cnt * M; e += T) {
     const uint32_t l = fdiv(e, L.dM), m = e - l * M;
@@ -173,7 +206,7 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
     r1[l * LD + pidx<PAD>(m)] = v;
   }
   __syncthreads();
-  const c32* r2 = fft_lines_smem<float>(r1, o1, L.sch, cnt, LD, tid, T, nullptr);
+  const c32* r2 = fft_lines_smem<float>(r1, o1, L.sch, cnt, LD, tid, T, bp.tw);
   const float sc = L.scale;
   for (uint32_t e = tid; e < cnt * N; e += T) {
     const uint32_t c = fdiv(e, L.dN), k = e - c * N;
@@ -186,9 +219,76 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
   }
 }
 
+// A long smooth line in one CTA: n = N2*n1 + n2, k = k1 + N1*k2.
+// Pass 1 takes kLongG adjacent columns n2 at a time, FFT_N1 over n1, the
+// W_N^{n2 k1} twiddle, into the CTA's scratch slot at N2*k1 + n2; pass 2
+// takes kLongG rows k1, FFT_N2 over n2, and writes X[k1 + N1*k2] (kLongG
+// consecutive outputs per k2).  The slot is reused line after line, so it
+// stays in L2.
+constexpr uint32_t kLongG = 8;
+
+FFT_D void batch_long(const BatchParams& bp, const BatchLen& L, int64_t base, c32* slot, c32* A,
+                      c32* B, uint32_t tid, uint32_t T) {
+  constexpr int PAD = PadOf<float>::value;
+  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2;
+  const bool inv = bp.inverse;
+  constexpr uint32_t G = kLongG;
+  for (uint32_t c0 = 0; c0 < N2; c0 += G) {
+    for (uint32_t e = tid; e < G * N1; e += T) {
+      const uint32_t n1 = e / G, c = e % G;
+      if (c0 + c < N2) cp_async8(&A[c * L.LD1 + pidx<PAD>(n1)], &bp.in[base + (int64_t)N2 * n1 + c0 + c]);
+      else A[c * L.LD1 + pidx<PAD>(n1)] = czero<float>();
+    }
+    cp_async_wait_all();
+    if (inv) {
+      for (uint32_t e = tid; e < G * N1; e += T) {
+        const uint32_t n1 = e / G, c = e % G;
+        c32& v = A[c * L.LD1 + pidx<PAD>(n1)];
+        v.im = -v.im;
+      }
+    }
+    __syncthreads();
+    const c32* r = fft_lines_smem<float>(A, B, L.sch, G, L.LD1, tid, T, bp.tw);
+    for (uint32_t e = tid; e < G * N1; e += T) {
+      const uint32_t k1 = e / G, c = e % G;
+      if (c0 + c < N2) {
+        c32 v = r[c * L.LD1 + pidx<PAD>(k1)];
+        v = cmul(v, tw2(bp, L, (c0 + c) * k1, N2));
+        slot[(uint64_t)N2 * k1 + c0 + c] = v;
+      }
+    }
+    __syncthreads();
+  }
+  const float sc = L.scale;
+  for (uint32_t k0 = 0; k0 < N1; k0 += G) {
+#pragma unroll 1
+    for (uint32_t rr = 0; rr < G; ++rr) {
+      const bool ok = k0 + rr < N1;
+      const c32* row = slot + (uint64_t)N2 * (k0 + rr);
+      for (uint32_t n2 = tid; n2 < N2; n2 += T) {
+        if (ok) cp_async8(&A[rr * L.LD2 + pidx<PAD>(n2)], &row[n2]);
+        else A[rr * L.LD2 + pidx<PAD>(n2)] = czero<float>();
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const c32* r = fft_lines_smem<float>(A, B, L.sch2, G, L.LD2, tid, T, bp.tw);
+    for (uint32_t e = tid; e < G * N2; e += T) {
+      const uint32_t k2 = e / G, rr = e % G;
+      if (k0 + rr < N1) {
+        c32 v = r[rr * L.LD2 + pidx<PAD>(k2)];
+        v.re *= sc;
+        v.im = inv ? -v.im * sc : v.im * sc;
+        bp.out[base + k0 + rr + (int64_t)N1 * k2] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Persistent CTA kernel: blockDim.x threads, dynamic shared memory holds the
 // two line buffers of the largest task plus Rader's x0/X0 slots.
-__global__ void __launch_bounds__(256) k_batch_cta(const __grid_constant__ BatchParams bp,
+__global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ BatchParams bp,
                                                    uint32_t buf_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BatchLen s_len;
@@ -212,6 +312,10 @@ __global__ void __launch_bounds__(256) k_batch_cta(const __grid_constant__ Batch
       case BK_MIXED: batch_mixed(bp, s_len, s_base, task.count, A, B, tid, T); break;
       case BK_RADER: batch_rader(bp, s_len, s_base, task.count, A, B, x0s, X0s, tid, T); break;
       case BK_BLUE: batch_blue(bp, s_len, s_base, task.count, A, B, tid, T); break;
+      case BK_LONG:
+        batch_long(bp, s_len, s_base[0], bp.scratch + (uint64_t)blockIdx.x * bp.slot_elems, A, B,
+                   tid, T);
+        break;
       default: break;
     }
     __syncthreads();
@@ -222,7 +326,7 @@ __global__ void __launch_bounds__(256) k_batch_cta(const __grid_constant__ Batch
 template <int P>
 FFT_D void cluster_radix_p(cooperative_groups::cluster_group& cl, c32* src_local, c32* dst_local,
                            uint32_t Lr, uint32_t Mt, uint32_t rank, uint32_t tid, uint32_t T,
-                           bool twiddle_first) {
+                           bool twiddle_first, const BatchParams& bp, const BatchLen& L) {
   // For m in this CTA's share: v[r] = src[r][m]; (twiddle_first: v[r] *= W_Mt^{m r});
   // DFT_P; (else: v[k2] *= W_Mt^{m k2}); dst[k2][m] = v[k2].
   constexpr int PAD = PadOf<float>::value;
@@ -235,12 +339,12 @@ FFT_D void cluster_radix_p(cooperative_groups::cluster_group& cl, c32* src_local
     for (int r = 0; r < P; ++r) v[r] = cl.map_shared_rank(src_local, r)[pm];
     if (twiddle_first) {
 #pragma unroll
-      for (int r = 1; r < P; ++r) v[r] = cmul(v[r], twiddle_f32((uint64_t)m * r, Mt));
+      for (int r = 1; r < P; ++r) v[r] = cmul(v[r], tw2(bp, L, m * r, Lr));
     }
     dft<float, P>(v);
     if (!twiddle_first) {
 #pragma unroll
-      for (int r = 1; r < P; ++r) v[r] = cmul(v[r], twiddle_f32((uint64_t)m * r, Mt));
+      for (int r = 1; r < P; ++r) v[r] = cmul(v[r], tw2(bp, L, m * r, Lr));
     }
 #pragma unroll
     for (int r = 0; r < P; ++r) cl.map_shared_rank(dst_local, r)[pm] = v[r];
@@ -291,20 +395,20 @@ __global__ void __launch_bounds__(512, 1) k_batch_cluster(const __grid_constant_
     cl.sync();
     // 2. cross-CTA radix-P step, twiddle after: A (all ranks) -> B (all ranks)
     if (L.P == P) {
-      cluster_radix_p<P>(cl, A, B, Lr, Mt, rank, tid, T, false);
+      cluster_radix_p<P>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L);
     } else if (active) {
       switch (L.P) {
-        case 2: cluster_radix_p<2>(cl, A, B, Lr, Mt, rank, tid, T, false); break;
-        case 3: cluster_radix_p<3>(cl, A, B, Lr, Mt, rank, tid, T, false); break;
-        case 4: cluster_radix_p<4>(cl, A, B, Lr, Mt, rank, tid, T, false); break;
-        case 5: cluster_radix_p<5>(cl, A, B, Lr, Mt, rank, tid, T, false); break;
-        case 7: cluster_radix_p<7>(cl, A, B, Lr, Mt, rank, tid, T, false); break;
+        case 2: cluster_radix_p<2>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L); break;
+        case 3: cluster_radix_p<3>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L); break;
+        case 4: cluster_radix_p<4>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L); break;
+        case 5: cluster_radix_p<5>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L); break;
+        case 7: cluster_radix_p<7>(cl, A, B, Lr, Mt, rank, tid, T, false, bp, L); break;
         default: break;
       }
     }
     cl.sync();
     // 3. local FFT_L of B (every rank runs it so barriers match; idle ranks on garbage)
-    c32* r = fft_lines_smem<float>(B, A, L.sch, 1, L.LD, tid, T, nullptr);
+    c32* r = fft_lines_smem<float>(B, A, L.sch, 1, L.LD, tid, T, bp.tw);
     c32* o = (r == A) ? B : A;
     if (!blue) {
       cl.sync();
@@ -334,19 +438,19 @@ __global__ void __launch_bounds__(512, 1) k_batch_cluster(const __grid_constant_
     }
     __syncthreads();
     // inverse in the mirrored order: local FFT_L first ...
-    c32* r2 = fft_lines_smem<float>(r, o, L.sch, 1, L.LD, tid, T, nullptr);
+    c32* r2 = fft_lines_smem<float>(r, o, L.sch, 1, L.LD, tid, T, bp.tw);
     c32* o2 = (r2 == r) ? o : r;
     cl.sync();
     // ... then the twiddle and the cross-CTA radix-P step: r2 -> o2
     if (L.P == P) {
-      cluster_radix_p<P>(cl, r2, o2, Lr, Mt, rank, tid, T, true);
+      cluster_radix_p<P>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L);
     } else if (active) {
       switch (L.P) {
-        case 2: cluster_radix_p<2>(cl, r2, o2, Lr, Mt, rank, tid, T, true); break;
-        case 3: cluster_radix_p<3>(cl, r2, o2, Lr, Mt, rank, tid, T, true); break;
-        case 4: cluster_radix_p<4>(cl, r2, o2, Lr, Mt, rank, tid, T, true); break;
-        case 5: cluster_radix_p<5>(cl, r2, o2, Lr, Mt, rank, tid, T, true); break;
-        case 7: cluster_radix_p<7>(cl, r2, o2, Lr, Mt, rank, tid, T, true); break;
+        case 2: cluster_radix_p<2>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L); break;
+        case 3: cluster_radix_p<3>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L); break;
+        case 4: cluster_radix_p<4>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L); break;
+        case 5: cluster_radix_p<5>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L); break;
+        case 7: cluster_radix_p<7>(cl, r2, o2, Lr, Mt, rank, tid, T, true, bp, L); break;
         default: break;
       }
     }

@@ -479,7 +479,6 @@ static cudaError_t prepare(K kernel, size_t smem) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (smem <= 48 * 1024) return cudaSuccess;
   const std::pair<const void*, int> key((const void*)kernel, dev);
   std::lock_guard<std::mutex> lk(mu);
   if (done.count(key)) return cudaSuccess;
