@@ -200,6 +200,31 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const v
 /* Task and launch summary as JSON (same length convention as the plan's). */
 b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_t* len);
 
+/* ---------------------------------------------------- allocation-free */
+
+/* No counterpart in the crate.  For callers that cannot allocate device
+ * memory -- code recording a CUDA graph whose capture forbids allocation, a
+ * plug-in running inside a host application that owns a fixed device-memory
+ * budget, a real-time path that must not take the allocator's locks or wait
+ * on its synchronisation -- this transforms `batch` 1D complex f32 lines of
+ * n points (n 2,3,5,7,11,13-smooth) from `in` to `out` without any
+ * allocation: no plan object, no tables (stage twiddles are computed in the
+ * kernels), and lines too long for one CTA run their two four-step passes
+ * through a static device array of 32 MiB inside the library.  Limit: the
+ * multi-pass route takes n * batch <= 4,194,304 points (32 MiB of f32
+ * complex); above it the call returns B2F_ERR_WORKSPACE_TOO_SMALL.  Every
+ * GPU that loads the library holds the 32 MiB array until the process
+ * exits.  The first call on each device looks the array's device address
+ * up (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture.  All calls share the one array (the last
+ * call's contents stay in it; every element is rewritten before it is read,
+ * so nothing needs clearing), so calls that overlap on the GPU race: issue
+ * them on one stream, or order them.  Inputs, outputs, direction and
+ * normalization are the caller's, as in b2f_plan_execute_checked. */
+b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint64_t in_bytes, void* out,
+                                  uint64_t out_bytes, uint64_t n, uint64_t batch,
+                                  int32_t direction, int32_t normalization);
+
 /* --------------------------------------------------------------- errors */
 
 /* FftError's Display (src/error.rs): a fixed name for each status. */
