@@ -22,6 +22,17 @@ cudaError_t launch_scale_copy_t(const void*, void*, uint64_t, double, bool, cuda
 template <class S>
 cudaError_t launch_blue_elem_t(const BlueElemParams&, cudaStream_t);
 
+template <class S>
+cudaError_t launch_real_elem_t(const RealElemParams&, cudaStream_t);
+
+cudaError_t launch_real_elem(Prec p, const RealElemParams& prm, cudaStream_t st) {
+  switch (p) {
+    case PREC_F32: return launch_real_elem_t<float>(prm, st);
+    case PREC_F64: return launch_real_elem_t<double>(prm, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_blue_elem(Prec p, const BlueElemParams& prm, cudaStream_t st) {
   switch (p) {
     case PREC_F32: return launch_blue_elem_t<float>(prm, st);

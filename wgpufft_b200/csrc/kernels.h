@@ -82,6 +82,19 @@ struct BlueElemParams {
   double scale;
 };
 
+// Generic real transforms (any N0): axis-0 lines expanded to full complex
+// lines, transformed by any complex route, then packed (R2C); or the
+// Hermitian mirror of the packed half, an inverse complex route, the real
+// part (C2R).  Lines are contiguous: real line r at r*N0, packed at r*P,
+// complex line at r*N0.
+enum RealElemMode : uint32_t { RE_EXPAND = 0, RE_PACK = 1, RE_UNPACK = 2, RE_TAKE_REAL = 3 };
+struct RealElemParams {
+  const void* in;
+  void* out;
+  uint32_t N0, P, mode, pad;
+  uint64_t nlines;
+};
+
 // Real transforms on axis 0 (contiguous lines; batches and the other axes
 // are `nlines` lines, real line r at r*N0 floats, packed line at r*(N0/2+1)).
 struct RealParams {
@@ -111,6 +124,7 @@ cudaError_t launch_r2c(Prec p, const RealParams& prm, unsigned grid, unsigned th
 cudaError_t launch_c2r(Prec p, const RealParams& prm, unsigned grid, unsigned threads,
                        size_t smem, cudaStream_t st);
 cudaError_t launch_blue_elem(Prec p, const BlueElemParams& prm, cudaStream_t st);
+cudaError_t launch_real_elem(Prec p, const RealElemParams& prm, cudaStream_t st);
 // out[i] = scale * (conj?) in[i] for n complex values (length-1 transforms).
 cudaError_t launch_scale_copy(Prec p, const void* in, void* out, uint64_t n, double scale,
                               bool conj, cudaStream_t st);

@@ -20,4 +20,5 @@ template cudaError_t launch_pow2_t<float, 16, false>(const LinesParams&, unsigne
 template cudaError_t launch_pow2_t<float, 16, true>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_pow2_t<float, 32, false>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_pow2_t<float, 32, true>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
+template cudaError_t launch_real_elem_t<float>(const RealElemParams&, cudaStream_t);
 }  // namespace b2f

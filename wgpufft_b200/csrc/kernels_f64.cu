@@ -18,4 +18,5 @@ template cudaError_t launch_c2r_t<double>(const RealParams&, unsigned, unsigned,
 template cudaError_t launch_blue_elem_t<double>(const BlueElemParams&, cudaStream_t);
 template cudaError_t launch_pow2_t<double, 16, false>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_pow2_t<double, 16, true>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
+template cudaError_t launch_real_elem_t<double>(const RealElemParams&, cudaStream_t);
 }  // namespace b2f

@@ -458,6 +458,36 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
 }
 
 template <class S>
+__global__ void __launch_bounds__(256) k_real_elem(const __grid_constant__ RealElemParams p) {
+  const uint32_t tid = threadIdx.x, T = blockDim.x;
+  const uint32_t N0 = p.N0, P = p.P;
+  for (uint64_t l = blockIdx.x; l < p.nlines; l += gridDim.x) {
+    if (p.mode == RE_EXPAND) {
+      const S* __restrict__ in = (const S*)p.in + l * N0;
+      C<S>* __restrict__ out = (C<S>*)p.out + l * N0;
+      for (uint32_t n = tid; n < N0; n += T) out[n] = {in[n], Scalar<S>::zero()};
+    } else if (p.mode == RE_PACK) {
+      const C<S>* __restrict__ in = (const C<S>*)p.in + l * N0;
+      C<S>* __restrict__ out = (C<S>*)p.out + l * P;
+      for (uint32_t k = tid; k < P; k += T) out[k] = in[k];
+    } else if (p.mode == RE_UNPACK) {
+      const C<S>* __restrict__ in = (const C<S>*)p.in + l * P;
+      C<S>* __restrict__ out = (C<S>*)p.out + l * N0;
+      for (uint32_t k = tid; k < N0; k += T) {
+        // X[k] for k < P; X[N0-k] = conj(X[k]) above; DC and Nyquist real
+        C<S> v = (k < P) ? in[k] : conj(in[N0 - k]);
+        if (k == 0 || 2 * k == N0) v.im = Scalar<S>::zero();
+        out[k] = v;
+      }
+    } else {
+      const C<S>* __restrict__ in = (const C<S>*)p.in + l * N0;
+      S* __restrict__ out = (S*)p.out + l * N0;
+      for (uint32_t n = tid; n < N0; n += T) out[n] = in[n].re;
+    }
+  }
+}
+
+template <class S>
 __global__ void k_scale_copy(const C<S>* __restrict__ in, C<S>* __restrict__ out, uint64_t n,
                              double scale, int conj_flag) {
   const S sc = Scalar<S>::from_double(scale);
@@ -529,6 +559,14 @@ cudaError_t launch_blue_elem_t(const BlueElemParams& prm, cudaStream_t st) {
   uint64_t blocks = prm.nlines < 148ull * 16 ? prm.nlines : 148ull * 16;
   if (blocks == 0) blocks = 1;
   k_blue_elem<S><<<(unsigned)blocks, 256, 0, st>>>(prm);
+  return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t launch_real_elem_t(const RealElemParams& prm, cudaStream_t st) {
+  uint64_t blocks = prm.nlines < 148ull * 16 ? prm.nlines : 148ull * 16;
+  if (blocks == 0) blocks = 1;
+  k_real_elem<S><<<(unsigned)blocks, 256, 0, st>>>(prm);
   return cudaGetLastError();
 }
 

@@ -45,7 +45,8 @@ static b2f_status noalloc_scratch(int dev, void** out) {
 
 static b2f_status noalloc_run(const Plan& plan, cudaStream_t st, const void* in, void* out,
                               void* const* ws) {
-  void* bufs[2 + kNumWorkspaces] = {const_cast<void*>(in), out, ws[0], ws[1], ws[2], ws[3]};
+  void* bufs[2 + kNumWorkspaces] = {const_cast<void*>(in), out};
+  for (int i = 0; i < kNumWorkspaces; ++i) bufs[2 + i] = ws[i];
   cudaError_t e = cudaSuccess;
   for (const Pass& p0 : plan.passes) {
     Pass p = p0;
@@ -119,7 +120,7 @@ extern "C" b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint6
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return fail(B2F_ERR_DEVICE, "no current device");
   void* scratch = nullptr;
-  void* ws[kNumWorkspaces] = {nullptr, nullptr, nullptr, nullptr};
+  void* ws[kNumWorkspaces] = {};
   if (need > 0) {
     st = noalloc_scratch(dev, &scratch);
     if (st) return st;

@@ -949,6 +949,56 @@ static b2f_status add_real_pass(Builder& b, bool r2c, uint64_t N0, uint64_t nlin
   return B2F_OK;
 }
 
+// Whether the fused axis-0 real pass can run N0 (even N0 with N0/2 13-smooth,
+// or odd 13-smooth N0, within one CTA).
+static bool real_fast_path(const Builder& b, uint64_t N0) {
+  const bool even = N0 % 2 == 0;
+  const uint64_t nfft = even ? N0 / 2 : N0;
+  const uint64_t nbuf = even ? N0 / 2 + 1 : N0;
+  return !stage_radices(nfft).empty() && b.fits_one_cta(nbuf) && N0 >= 2;
+}
+
+static Pass real_elem_pass(RealElemMode mode, uint64_t N0, uint64_t nlines, int src, int dst,
+                           const char* label) {
+  Pass ps;
+  ps.kind = Pass::REAL_ELEM;
+  ps.axis = 0;
+  ps.src = src;
+  ps.dst = dst;
+  ps.label = label;
+  ps.route = "real";
+  ps.relem = RealElemParams{nullptr, nullptr, (uint32_t)N0, (uint32_t)(N0 / 2 + 1), mode, 0, nlines};
+  return ps;
+}
+
+// R2C axis 0 for any N0: expand to complex lines, complex FFT (any route),
+// keep the first N0/2+1 bins.
+static b2f_status add_real_generic_r2c(Builder& b, uint64_t N0, uint64_t nlines, bool last,
+                                       double scale) {
+  b.need(BUF_WS4, N0 * nlines * b.cb());
+  b.plan.passes.push_back(real_elem_pass(RE_EXPAND, N0, nlines, BUF_IN, BUF_WS4, "r2c-expand-stage"));
+  int cur = BUF_WS4;
+  b2f_status st = add_complex_axis(b, 0, axis_kind_for(b.plan.cfg, 0), N0, 1, nlines, true, last,
+                                   scale, &cur, BUF_WS4, BUF_WS5, false);
+  if (st) return st;
+  b.plan.passes.push_back(real_elem_pass(RE_PACK, N0, nlines, BUF_WS4, BUF_OUT, "r2c-pack-stage"));
+  return B2F_OK;
+}
+
+// C2R axis 0 for any N0: Hermitian mirror into complex lines, inverse
+// complex FFT (any route), real part.
+static b2f_status add_real_generic_c2r(Builder& b, uint64_t N0, uint64_t nlines, double scale,
+                                       int src) {
+  b.need(BUF_WS4, N0 * nlines * b.cb());
+  b.plan.passes.push_back(real_elem_pass(RE_UNPACK, N0, nlines, src, BUF_WS4, "c2r-unpack-stage"));
+  int cur = BUF_WS4;
+  b2f_status st = add_complex_axis(b, 0, axis_kind_for(b.plan.cfg, 0), N0, 1, nlines, true, true,
+                                   scale, &cur, BUF_WS4, BUF_WS5, true);
+  if (st) return st;
+  b.plan.passes.push_back(real_elem_pass(RE_TAKE_REAL, N0, nlines, BUF_WS4, BUF_OUT, "c2r-take-real-stage"));
+  return B2F_OK;
+}
+
 Plan::~Plan() {
   int prev = -1;
   cudaGetDevice(&prev);
@@ -994,7 +1044,8 @@ static void build_diagnostics(Plan& plan) {
     const Pass& p = plan.passes[i];
     const char* kind = p.kind == Pass::LINES ? "lines" : p.kind == Pass::POW2 ? (p.colmajor ? "register-pow2-columns" : "register-pow2-lines") : p.kind == Pass::RADER ? "rader"
                      : p.kind == Pass::BLUESTEIN ? "bluestein" : p.kind == Pass::R2C ? "r2c"
-                     : p.kind == Pass::C2R ? "c2r" : p.kind == Pass::BLUE_ELEM ? "bluestein-elementwise" : "scale-copy";
+                     : p.kind == Pass::C2R ? "c2r" : p.kind == Pass::BLUE_ELEM ? "bluestein-elementwise"
+                     : p.kind == Pass::REAL_ELEM ? "real-elementwise" : "scale-copy";
     uint32_t G = (p.kind == Pass::LINES || p.kind == Pass::POW2) ? p.lines.G : p.kind == Pass::RADER ? p.rader.L.G
                : p.kind == Pass::BLUESTEIN ? p.blue.L.G : (p.kind == Pass::R2C || p.kind == Pass::C2R) ? p.real.G : 0;
     os << (i ? "," : "") << "{\"label\":\"" << json_escape(p.label) << "\",\"kind\":\"" << kind
@@ -1123,7 +1174,10 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
     if (kind == B2F_R2C) {
       plan->in_bytes = total * sbytes;
       plan->out_bytes = ptotal * cbytes;
-      st = add_real_pass(b, true, N0, nlines, scale, rank == 1 && scale != 1.0, BUF_IN, BUF_OUT);
+      if (real_fast_path(b, N0))
+        st = add_real_pass(b, true, N0, nlines, scale, rank == 1 && scale != 1.0, BUF_IN, BUF_OUT);
+      else
+        st = add_real_generic_r2c(b, N0, nlines, rank == 1, scale);
       if (st) return st;
       int cur = BUF_OUT;
       for (int a = 1; a < rank; ++a) {
@@ -1146,7 +1200,10 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
                               1.0, &cur, BUF_WS0, BUF_WS1, true);
         if (st) return st;
       }
-      st = add_real_pass(b, false, N0, nlines, scale, scale != 1.0, cur, BUF_OUT);
+      if (real_fast_path(b, N0))
+        st = add_real_pass(b, false, N0, nlines, scale, scale != 1.0, cur, BUF_OUT);
+      else
+        st = add_real_generic_c2r(b, N0, nlines, scale, cur);
       if (st) return st;
     }
   }
@@ -1186,7 +1243,8 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
 // ------------------------------------------------------------ execution
 static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, void* out) {
   if (plan.device < 0) return fail(B2F_ERR_DEVICE, "plan was created for planning only (no device)");
-  void* bufs[2 + kNumWorkspaces] = {const_cast<void*>(in), out, plan.ws[0], plan.ws[1], plan.ws[2], plan.ws[3]};
+  void* bufs[2 + kNumWorkspaces] = {const_cast<void*>(in), out};
+  for (int i = 0; i < kNumWorkspaces; ++i) bufs[2 + i] = plan.ws[i];
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != plan.device) cudaSetDevice(plan.device);
@@ -1233,6 +1291,11 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
         p.belem.in = src;
         p.belem.out = dst;
         e = launch_blue_elem(plan.prec, p.belem, st);
+        break;
+      case Pass::REAL_ELEM:
+        p.relem.in = src;
+        p.relem.out = dst;
+        e = launch_real_elem(plan.prec, p.relem, st);
         break;
     }
     if (e != cudaSuccess) break;

@@ -52,11 +52,13 @@ enum class AxisKind { Mixed, Rader, Bluestein };
 enum class Route { DirectDft, MixedRadix, Rader, Bluestein, AxisSequence };
 
 // Buffers a pass reads or writes.
-enum BufId : int { BUF_IN = 0, BUF_OUT = 1, BUF_WS0 = 2, BUF_WS1 = 3, BUF_WS2 = 4, BUF_WS3 = 5 };
-constexpr int kNumWorkspaces = 4;
+enum BufId : int {
+  BUF_IN = 0, BUF_OUT = 1, BUF_WS0 = 2, BUF_WS1 = 3, BUF_WS2 = 4, BUF_WS3 = 5, BUF_WS4 = 6, BUF_WS5 = 7
+};
+constexpr int kNumWorkspaces = 6;
 
 struct Pass {
-  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM } kind = LINES;
+  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM, REAL_ELEM } kind = LINES;
   int pow2_E = 16;         // POW2: values per thread
   bool colmajor = false;   // POW2: adjacent lines first
   std::string label;  // stage label (diagnostics)
@@ -71,6 +73,7 @@ struct Pass {
   BluesteinParams blue{};
   RealParams real{};
   BlueElemParams belem{};
+  RealElemParams relem{};
   uint64_t copy_n = 0;
   double copy_scale = 1.0;
   bool copy_conj = false;
@@ -88,8 +91,8 @@ struct Plan {
   std::vector<Pass> passes;
   std::vector<void*> device_allocs;
   uint64_t table_bytes = 0;
-  void* ws[kNumWorkspaces] = {nullptr, nullptr, nullptr, nullptr};
-  uint64_t ws_bytes[kNumWorkspaces] = {0, 0, 0, 0};
+  void* ws[kNumWorkspaces] = {};
+  uint64_t ws_bytes[kNumWorkspaces] = {};
   uint64_t workspace_total() const {
     uint64_t t = 0;
     for (auto b : ws_bytes) t += b;
