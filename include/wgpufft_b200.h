@@ -184,6 +184,14 @@ typedef struct b2f_batch b2f_batch;
 b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
                          uint64_t count, int32_t direction, int32_t normalization,
                          int32_t device);
+/* b2f_batch_new with flags: bit 0 (B2F_BATCH_CLUSTERS) runs lines too long
+ * for one CTA on 8/16-CTA thread-block clusters that keep the whole line in
+ * distributed shared memory (one HBM pass, fewer lines in flight) instead
+ * of the default two-pass per-CTA route through L2-resident scratch. */
+#define B2F_BATCH_CLUSTERS 1u
+b2f_status b2f_batch_new_ex(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
+                            uint64_t count, int32_t direction, int32_t normalization,
+                            int32_t device, uint32_t flags);
 void b2f_batch_free(b2f_batch* batch);
 /* Bytes each of the input and output buffers must hold. */
 uint64_t b2f_batch_required_buffer_size_bytes(const b2f_batch* batch);

@@ -10,13 +10,15 @@ from wgpufft_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def run_batch(lengths, inverse=False, norm=w.Normalization.Inverse, in_place=False, seed=1):
+def run_batch(lengths, inverse=False, norm=w.Normalization.Inverse, in_place=False, seed=1,
+              clusters=False):
     import torch
     lengths = np.asarray(lengths, dtype=np.int64)
     off = W.packed_offsets(lengths)
     total = int(lengths.sum())
     x = W.normal_complex(total, seed)
-    b = w.FftBatch(lengths, off, w.FftDirection.Inverse if inverse else w.FftDirection.Forward, norm)
+    b = w.FftBatch(lengths, off, w.FftDirection.Inverse if inverse else w.FftDirection.Forward, norm,
+                   clusters=clusters)
     dx = torch.from_numpy(x.view(np.float32)).cuda()
     if in_place:
         b.execute(dx, dx)
@@ -49,9 +51,20 @@ SMALL = [16, 17, 31, 32, 34, 97, 100, 127, 128, 243, 256, 360, 1000, 1009, 1024,
 def test_batch_lengths_match_oracle(cuda):
     lengths = np.array(SMALL * 2)
     x, y, off, b = run_batch(lengths)
-    d = b.diagnostics()
-    assert d["cluster_lines"] > 0 and d["cta_lines"] > 0
+    k = b.diagnostics()["kind_lines"]
+    assert k["two_pass"] > 0 and k["two_pass_bluestein"] > 0 and k["mixed"] > 0
+    assert k["rader"] > 0 and k["bluestein"] > 0
     check_lines(x, y, lengths, off, range(len(lengths)))
+
+
+def test_batch_cluster_route_matches_oracle(cuda):
+    # the distributed-shared-memory route for long lines (8/16-CTA clusters)
+    lengths = np.array(SMALL)
+    x, y, off, b = run_batch(lengths, clusters=True, seed=9)
+    assert b.diagnostics()["cluster_lines"] > 0
+    check_lines(x, y, lengths, off, range(len(lengths)))
+    x, y, off, b = run_batch(lengths, clusters=True, inverse=True, seed=10)
+    check_lines(x, y, lengths, off, range(len(lengths)), inverse=True)
 
 
 def test_batch_inverse_and_normalisations(cuda):

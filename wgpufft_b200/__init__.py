@@ -90,6 +90,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_recorder_submit": (st, [vp, vp]),
         "b2f_recorder_free": (None, [vp]),
         "b2f_batch_new": (st, [pvp, ctypes.POINTER(u64), ctypes.POINTER(u64), u64, i32, i32, i32]),
+        "b2f_batch_new_ex": (st, [pvp, ctypes.POINTER(u64), ctypes.POINTER(u64), u64, i32, i32, i32,
+                                 u32]),
         "b2f_batch_free": (None, [vp]),
         "b2f_batch_required_buffer_size_bytes": (u64, [vp]),
         "b2f_batch_execute": (st, [vp, vp, vp, u64, vp, u64]),
@@ -520,14 +522,16 @@ class FftBatch:
     (b2f_batch_*): line i has lengths[i] points at complex offset offsets[i]."""
 
     def __init__(self, lengths, offsets, direction=FftDirection.Forward,
-                 normalization=Normalization.Inverse, device: Optional[int] = None):
+                 normalization=Normalization.Inverse, device: Optional[int] = None,
+                 clusters: bool = False):
         L = lib()
         n = len(lengths)
         la = (ctypes.c_uint64 * n)(*[int(x) for x in lengths])
         oa = (ctypes.c_uint64 * n)(*[int(x) for x in offsets])
         self._ptr = ctypes.c_void_p()
-        _check(L.b2f_batch_new(ctypes.byref(self._ptr), la, oa, n, int(direction),
-                               int(normalization), -1 if device is None else int(device)))
+        _check(L.b2f_batch_new_ex(ctypes.byref(self._ptr), la, oa, n, int(direction),
+                                  int(normalization), -1 if device is None else int(device),
+                                  1 if clusters else 0))
         self.count = n
 
     def required_buffer_size_bytes(self) -> int:

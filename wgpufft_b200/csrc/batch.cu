@@ -104,7 +104,7 @@ struct BatchPlan {
   c32* d_tw = nullptr;
   uint64_t tw_bytes = 0;
   uint64_t scratch_bytes = 0;
-  uint64_t kind_lines[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t kind_lines[7] = {0, 0, 0, 0, 0, 0, 0};
   std::string diag;
   ~BatchPlan() {
     int prev = -1;
@@ -138,7 +138,7 @@ struct LenInfo {
 
 // Chooses the execution of one distinct length.
 static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_t cta_cap,
-                     size_t cl_cap, LenInfo& li) {
+                     size_t cl_cap, bool clusters, LenInfo& li) {
   BatchLen& d = li.d;
   std::memset(&d, 0, sizeof(d));
   d.N = (uint32_t)N;
@@ -151,19 +151,40 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   d.scale = sc;
   d.dN = make_fastdiv((uint32_t)N);
   const auto cta_bytes = [](uint64_t lbuf) { return 2 * (size_t)ld_f32(lbuf) * 8; };
-  // long smooth lines: two passes N = N1 * N2 inside one CTA, both <= 256,
-  // as balanced as the divisors allow
-  uint64_t n1 = 0;
-  if (is_smooth13(N) && cta_bytes(N) > cta_cap) {
+  // long lines run as two passes of T = N1 * N2 (both <= 512) inside one
+  // CTA; the most balanced split of T, 0 when none exists
+  const auto split = [](uint64_t Tl) -> uint64_t {
+    uint64_t best_a = 0;
     double best = 1e300;
-    for (uint64_t a = 2; a <= 256; ++a) {
-      if (N % a || N / a > 256) continue;
-      const double bal = std::fabs(std::log((double)a) - std::log((double)(N / a)));
+    for (uint64_t a = 2; a <= 512; ++a) {
+      if (Tl % a || Tl / a > 512 || Tl / a < 2) continue;
+      const double bal = std::fabs(std::log((double)a) - std::log((double)(Tl / a)));
       if (bal < best) {
         best = bal;
-        n1 = a;
+        best_a = a;
       }
     }
+    return best_a;
+  };
+  uint64_t n1 = 0;
+  if (is_smooth13(N) && cta_bytes(N) > cta_cap && !clusters) n1 = split(N);
+  uint32_t cl_split = 0;
+  if (clusters && is_smooth13(N) && cta_bytes(N) > cta_cap)
+    for (uint32_t P : {8u, 7u, 5u, 4u, 3u, 2u})
+      if (N % P == 0 && cta_bytes(N / P) <= cl_cap) {
+        cl_split = P;
+        break;
+      }
+  if (cl_split) {
+    d.kind = BK_CL_MIXED;
+    d.M = (uint32_t)N;
+    d.P = cl_split;
+    d.L = (uint32_t)(N / cl_split);
+    d.LD = ld_f32(d.L);
+    d.sch = schedule_for(d.L);
+    d.G = 1;
+    li.cost = (double)N * std::log2((double)N);
+    return true;
   }
   const bool smooth = is_smooth13(N) && (cta_bytes(N) <= cta_cap || n1);
   if (smooth && cta_bytes(N) <= cta_cap) {
@@ -179,6 +200,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     d.LD1 = ld_f32(d.N1);
     d.LD2 = ld_f32(d.N2);
     d.LD = std::max(d.LD1, d.LD2);
+    d.lg = std::max(d.N1, d.N2) <= 256 ? 3 : 2;
     d.sch = schedule_for(d.N1);
     d.sch2 = schedule_for(d.N2);
   } else if (is_prime_u64(N) && N >= 3 && is_smooth13(N - 1) && cta_bytes(N) <= cta_cap) {
@@ -207,11 +229,35 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   } else {
     uint64_t M = 2 * N - 1;
     while (!smooth7(M)) ++M;
+    uint64_t mlong = 0, a = 0;
+    if (cta_bytes(M) > cta_cap && !clusters) {
+      // smallest 7-smooth convolution length that splits into two factors <= 512
+      for (uint64_t m = 2 * N - 1; m <= 262144; ++m) {
+        if (!smooth7(m)) continue;
+        a = split(m);
+        if (a) {
+          mlong = m;
+          break;
+        }
+      }
+    }
     if (cta_bytes(M) <= cta_cap) {
       d.kind = BK_BLUE;
       d.M = (uint32_t)M;
       d.LD = ld_f32(M);
       d.sch = schedule_for(M);
+    } else if (mlong) {
+      M = mlong;
+      d.kind = BK_LONG_BLUE;
+      d.M = (uint32_t)M;
+      d.N1 = (uint32_t)a;
+      d.N2 = (uint32_t)(M / a);
+      d.LD1 = ld_f32(d.N1);
+      d.LD2 = ld_f32(d.N2);
+      d.LD = std::max(d.LD1, d.LD2);
+      d.lg = std::max(d.N1, d.N2) <= 256 ? 3 : 2;
+      d.sch = schedule_for(d.N1);
+      d.sch2 = schedule_for(d.N2);
     } else {
       // cluster Bluestein: convolution P*L >= 2N-1, L 7-smooth and fitting
       uint32_t P = kClusterP;
@@ -244,7 +290,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   }
   const double T = d.M;
   li.cost = T * std::log2(std::max(2.0, T)) * (d.kind == BK_BLUE || d.kind == BK_CL_BLUE ? 3 : 1);
-  if (d.kind == BK_LONG) {
+  if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
     d.G = 1;
   } else if (d.kind == BK_MIXED || d.kind == BK_RADER || d.kind == BK_BLUE) {
     uint64_t G = std::max<uint64_t>(1, 4096 / d.M);
@@ -266,7 +312,7 @@ static cudaError_t set_smem(K kernel, size_t smem) {
 
 static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets, uint64_t nlines,
                                int32_t direction, int32_t normalization, int device,
-                               BatchPlan** out) {
+                               uint32_t flags, BatchPlan** out) {
   *out = nullptr;
   if (!lengths || !offsets || nlines == 0) return fail(B2F_ERR_INVALID_ARGUMENT, "empty batch");
   if (direction != B2F_FORWARD && direction != B2F_INVERSE)
@@ -316,7 +362,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     for (unsigned w = 0; w < nth; ++w)
       th.emplace_back([&, w] {
         for (size_t i = w; i < lens_list.size(); i += nth)
-          ok[i] = classify(lens_list[i], direction, normalization, cta_cap, cl_cap, infos[i]);
+          ok[i] = classify(lens_list[i], direction, normalization, cta_cap, cl_cap,
+                           (flags & 1u) != 0, infos[i]);
       });
     for (auto& t : th) t.join();
   }
@@ -334,12 +381,12 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     for (auto& li : infos) {
       BatchLen& d = li.d;
       attach_stage_table(d.sch, tw, cache);
-      if (d.kind == BK_LONG) {
+      if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
         attach_stage_table(d.sch2, tw, cache);
         d.ta = (uint32_t)tw.size();
-        for (uint32_t a = 0; a < d.N1; ++a) tw.push_back(root_fwd((uint64_t)a * d.N2, d.N));
+        for (uint32_t a = 0; a < d.N1; ++a) tw.push_back(root_fwd((uint64_t)a * d.N2, d.M));
         d.tb = (uint32_t)tw.size();
-        for (uint32_t c = 0; c < d.N2; ++c) tw.push_back(root_fwd(c, d.N));
+        for (uint32_t c = 0; c < d.N2; ++c) tw.push_back(root_fwd(c, d.M));
         d.dB = make_fastdiv(d.N2);
       } else if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) {
         d.ta = (uint32_t)tw.size();
@@ -448,9 +495,11 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   for (auto& li : infos) {
     const BatchLen& d = li.d;
     if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) buf_cl = std::max(buf_cl, d.LD);
-    else if (d.kind == BK_LONG) buf_cta = std::max<uint32_t>(buf_cta, kLongG * d.LD);
+    else if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE)
+      buf_cta = std::max<uint32_t>(buf_cta, (1u << d.lg) * d.LD);
     else buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
     if (d.kind == BK_LONG) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, d.N);
+    if (d.kind == BK_LONG_BLUE) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, 2ull * d.M);
   }
   bp->buf_cta = buf_cta;
   bp->buf_cl = buf_cl;
@@ -544,7 +593,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
      << ",\"cta_tasks\":" << bp->n_cta << ",\"cluster_tasks\":" << bp->n_cl
      << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
      << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
-     << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5] << "}"
+     << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5]
+     << ",\"two_pass_bluestein\":" << bp->kind_lines[6] << "}"
      << ",\"scratch_bytes\":" << bp->scratch_bytes << ",\"twiddle_table_bytes\":" << bp->tw_bytes
      << ",\"cta_grid\":" << bp->grid_cta << ",\"cta_threads\":" << kCtaThreads
      << ",\"cta_smem\":" << bp->smem_cta << ",\"cluster_grid\":" << bp->grid_cl
@@ -636,16 +686,22 @@ struct b2f_batch {
 
 extern "C" {
 
-b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
-                         uint64_t nlines, int32_t direction, int32_t normalization,
-                         int32_t device) {
+b2f_status b2f_batch_new_ex(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
+                            uint64_t nlines, int32_t direction, int32_t normalization,
+                            int32_t device, uint32_t flags) {
   if (!out) return fail(B2F_ERR_INVALID_ARGUMENT, "null output handle");
   *out = nullptr;
   BatchPlan* p = nullptr;
-  b2f_status st = create_batch(lengths, offsets, nlines, direction, normalization, device, &p);
+  b2f_status st = create_batch(lengths, offsets, nlines, direction, normalization, device, flags, &p);
   if (st) return st;
   *out = new b2f_batch{p};
   return B2F_OK;
+}
+
+b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
+                         uint64_t nlines, int32_t direction, int32_t normalization,
+                         int32_t device) {
+  return b2f_batch_new_ex(out, lengths, offsets, nlines, direction, normalization, device, 0);
 }
 
 void b2f_batch_free(b2f_batch* b) {

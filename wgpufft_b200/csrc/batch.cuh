@@ -32,6 +32,7 @@ enum BatchKind : uint32_t {
   BK_CL_MIXED = 3,  // cluster, mixed radix (T = N)
   BK_CL_BLUE = 4,   // cluster, Bluestein (T = convolution length)
   BK_LONG = 5,      // one CTA, two passes N = N1*N2 through an L2-resident scratch slot
+  BK_LONG_BLUE = 6, // one CTA, Bluestein over M = N1*N2: four passes through two slots
 };
 
 struct BatchLen {
@@ -53,6 +54,7 @@ struct BatchLen {
   //   BK_LONG: T = N, B = N2 (a < N1);  cluster kinds: T = M, B = L (a < P).
   uint32_t ta, tb;
   FastDiv dB;
+  uint32_t lg;    // long kinds: log2 of the lines per pass group (G = 1 << lg)
   Schedule sch;   // schedule of the per-CTA FFT length (N, p-1, M, L or N1)
   Schedule sch2;  // BK_LONG: schedule of N2
 };
@@ -219,46 +221,74 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
   }
 }
 
-// A long smooth line in one CTA: n = N2*n1 + n2, k = k1 + N1*k2.
-// Pass 1 takes kLongG adjacent columns n2 at a time, FFT_N1 over n1, the
-// W_N^{n2 k1} twiddle, into the CTA's scratch slot at N2*k1 + n2; pass 2
-// takes kLongG rows k1, FFT_N2 over n2, and writes X[k1 + N1*k2] (kLongG
-// consecutive outputs per k2).  The slot is reused line after line, so it
-// stays in L2.
-constexpr uint32_t kLongG = 8;
+// Long lines in one CTA, through scratch slots (reused line after line, so
+// they mostly stay in L2).  One length-T = N1*N2 FFT is two passes with
+// n = N2*n1 + n2, k = k1 + N1*k2:
+//   column pass: G adjacent columns n2 at a time, FFT_N1 over n1, the
+//                W_T^{n2 k1} twiddle, stored at N2*k1 + n2;
+//   row pass:    G rows k1 at a time, FFT_N2 over n2, X[k1 + N1*k2] (G
+//                consecutive outputs per k2).
+// The hooks decide where a pass reads and writes: the input of the column
+// pass (a line of x, optionally chirped and zero-padded, or a slot) and the
+// output of the row pass (the line of out, or a slot in natural order after
+// the Bluestein spectrum product).
+enum LongIn : uint32_t { LI_X = 0, LI_X_CHIRP = 1, LI_SLOT = 2 };
+enum LongOut : uint32_t { LO_X = 0, LO_SLOT_SPECTRUM = 1, LO_X_CHIRP = 2 };
 
-FFT_D void batch_long(const BatchParams& bp, const BatchLen& L, int64_t base, c32* slot, c32* A,
-                      c32* B, uint32_t tid, uint32_t T) {
+FFT_D void long_column_pass(const BatchParams& bp, const BatchLen& L, int64_t base,
+                            const c32* src_slot, c32* dst, LongIn mode, c32* A, c32* B,
+                            uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<float>::value;
-  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2;
+  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2, lg = L.lg, G = 1u << lg;
   const bool inv = bp.inverse;
-  constexpr uint32_t G = kLongG;
   for (uint32_t c0 = 0; c0 < N2; c0 += G) {
-    for (uint32_t e = tid; e < G * N1; e += T) {
-      const uint32_t n1 = e / G, c = e % G;
-      if (c0 + c < N2) cp_async8(&A[c * L.LD1 + pidx<PAD>(n1)], &bp.in[base + (int64_t)N2 * n1 + c0 + c]);
-      else A[c * L.LD1 + pidx<PAD>(n1)] = czero<float>();
+    for (uint32_t e = tid; e < (N1 << lg); e += T) {
+      const uint32_t n1 = e >> lg, c = e & (G - 1);
+      c32* d = &A[c * L.LD1 + pidx<PAD>(n1)];
+      const uint32_t n = N2 * n1 + c0 + c;
+      if (c0 + c >= N2) {
+        *d = czero<float>();
+      } else if (mode == LI_SLOT) {
+        cp_async8(d, &src_slot[n]);
+      } else if (mode == LI_X) {
+        cp_async8(d, &bp.in[base + n]);
+      } else {  // chirped, zero beyond the line
+        if (n < N) {
+          c32 v = bp.in[base + n];
+          if (inv) v.im = -v.im;
+          *d = cmul(v, chirp<float>(n, N));
+        } else {
+          *d = czero<float>();
+        }
+      }
     }
     cp_async_wait_all();
-    if (inv) {
-      for (uint32_t e = tid; e < G * N1; e += T) {
-        const uint32_t n1 = e / G, c = e % G;
+    if (inv && mode == LI_X) {
+      for (uint32_t e = tid; e < (N1 << lg); e += T) {
+        const uint32_t n1 = e >> lg, c = e & (G - 1);
         c32& v = A[c * L.LD1 + pidx<PAD>(n1)];
         v.im = -v.im;
       }
     }
     __syncthreads();
     const c32* r = fft_lines_smem<float>(A, B, L.sch, G, L.LD1, tid, T, bp.tw);
-    for (uint32_t e = tid; e < G * N1; e += T) {
-      const uint32_t k1 = e / G, c = e % G;
+    for (uint32_t e = tid; e < (N1 << lg); e += T) {
+      const uint32_t k1 = e >> lg, c = e & (G - 1);
       if (c0 + c < N2) {
         c32 v = r[c * L.LD1 + pidx<PAD>(k1)];
         v = cmul(v, tw2(bp, L, (c0 + c) * k1, N2));
-        slot[(uint64_t)N2 * k1 + c0 + c] = v;
+        dst[(uint64_t)N2 * k1 + c0 + c] = v;
       }
     }
     __syncthreads();
   }
+}
+
+FFT_D void long_row_pass(const BatchParams& bp, const BatchLen& L, int64_t base, const c32* slot,
+                         c32* dst_slot, LongOut mode, c32* A, c32* B, uint32_t tid, uint32_t T) {
+  constexpr int PAD = PadOf<float>::value;
+  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2, lg = L.lg, G = 1u << lg;
+  const bool inv = bp.inverse;
   const float sc = L.scale;
   for (uint32_t k0 = 0; k0 < N1; k0 += G) {
 #pragma unroll 1
@@ -273,17 +303,49 @@ FFT_D void batch_long(const BatchParams& bp, const BatchLen& L, int64_t base, c3
     cp_async_wait_all();
     __syncthreads();
     const c32* r = fft_lines_smem<float>(A, B, L.sch2, G, L.LD2, tid, T, bp.tw);
-    for (uint32_t e = tid; e < G * N2; e += T) {
-      const uint32_t k2 = e / G, rr = e % G;
-      if (k0 + rr < N1) {
-        c32 v = r[rr * L.LD2 + pidx<PAD>(k2)];
+    for (uint32_t e = tid; e < (N2 << lg); e += T) {
+      const uint32_t k2 = e >> lg, rr = e & (G - 1);
+      if (k0 + rr >= N1) continue;
+      const uint32_t k = k0 + rr + N1 * k2;
+      c32 v = r[rr * L.LD2 + pidx<PAD>(k2)];
+      if (mode == LO_X) {
         v.re *= sc;
         v.im = inv ? -v.im * sc : v.im * sc;
-        bp.out[base + k0 + rr + (int64_t)N1 * k2] = v;
+        bp.out[base + k] = v;
+      } else if (mode == LO_SLOT_SPECTRUM) {
+        v = cmul(v, L.bhat[k]);
+        v.im = -v.im;  // conjugated: the next forward FFT computes the inverse
+        dst_slot[k] = v;
+      } else if (k < N) {
+        v.im = -v.im;
+        v = cmul(v, chirp<float>(k, N));
+        v.re *= sc;
+        v.im = inv ? -v.im * sc : v.im * sc;
+        bp.out[base + k] = v;
       }
     }
     __syncthreads();
   }
+}
+
+// A long smooth line: two passes through one slot.
+FFT_D void batch_long(const BatchParams& bp, const BatchLen& L, int64_t base, c32* slot, c32* A,
+                      c32* B, uint32_t tid, uint32_t T) {
+  long_column_pass(bp, L, base, nullptr, slot, LI_X, A, B, tid, T);
+  long_row_pass(bp, L, base, slot, nullptr, LO_X, A, B, tid, T);
+}
+
+// A long Bluestein line, convolution M = N1*N2: chirped column pass and row
+// pass into the spectrum product (slot 2, natural order, conjugated), then
+// the column and row passes of the second FFT, chirped into the output.
+FFT_D void batch_long_blue(const BatchParams& bp, const BatchLen& L, int64_t base, c32* slot,
+                           c32* A, c32* B, uint32_t tid, uint32_t T) {
+  c32* s1 = slot;
+  c32* s2 = slot + L.M;
+  long_column_pass(bp, L, base, nullptr, s1, LI_X_CHIRP, A, B, tid, T);
+  long_row_pass(bp, L, base, s1, s2, LO_SLOT_SPECTRUM, A, B, tid, T);
+  long_column_pass(bp, L, base, s2, s1, LI_SLOT, A, B, tid, T);
+  long_row_pass(bp, L, base, s1, nullptr, LO_X_CHIRP, A, B, tid, T);
 }
 
 // Persistent CTA kernel: blockDim.x threads, dynamic shared memory holds the
@@ -315,6 +377,10 @@ __global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ Ba
       case BK_LONG:
         batch_long(bp, s_len, s_base[0], bp.scratch + (uint64_t)blockIdx.x * bp.slot_elems, A, B,
                    tid, T);
+        break;
+      case BK_LONG_BLUE:
+        batch_long_blue(bp, s_len, s_base[0], bp.scratch + (uint64_t)blockIdx.x * bp.slot_elems,
+                        A, B, tid, T);
         break;
       default: break;
     }
