@@ -165,6 +165,88 @@ def cpu_sample_rate(lengths, offsets, x, seconds_target=10.0, threads=0):
         take = min(len(lengths), take * 3)
 
 
+def serving_measurement(local, count=300, rate=2000.0, max_bytes=8 << 20, seed=9):
+    """Open-loop Poisson stream of the serving configuration through the
+    serving loop (resident plans, admission, coalescing, 4 streams) against
+    the plain per-request path (its own plan, copies in, execute, copies out,
+    one request at a time), both with plans created beforehand."""
+    import threading
+
+    import torch
+    import wgpufft_b200 as w
+    from wgpufft_b200 import workloads as W
+
+    reqs = W.serving_requests(count, seed=seed, max_bytes=max_bytes)
+    rng = np.random.default_rng(seed + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+
+    def cfg_of(q):
+        c = w.FftConfig.new_nd(q["shape"]).with_batch(q["batch"]).with_precision(q["precision"])
+        return c.with_direction(w.FftDirection.Inverse if q["inverse"] else w.FftDirection.Forward)
+
+    cfgs = [cfg_of(q) for q in reqs]
+    kinds = [w.FftTransformKind(q["kind"]) for q in reqs]
+    plans = [{0: w.FftPlan.c2c, 1: w.FftPlan.r2c, 2: w.FftPlan.c2r}[int(k)](c, device=local)
+             for c, k in zip(cfgs, kinds)]
+    ins, outs = [], []
+    for p in plans:
+        ib, ob = p.required_input_buffer_size_bytes(), p.required_output_buffer_size_bytes()
+        ins.append(torch.zeros(ib // 4, dtype=torch.float32).pin_memory())
+        outs.append(torch.zeros(ob // 4, dtype=torch.float32).pin_memory())
+    transforms = sum(q["batch"] for q in reqs)
+    # plain per-request path
+    stream = torch.cuda.current_stream()
+    din = torch.empty(max(t.numel() for t in ins), dtype=torch.float32, device="cuda")
+    dout = torch.empty(max(t.numel() for t in outs), dtype=torch.float32, device="cuda")
+    for p, hi, ho in zip(plans[:8], ins, outs):  # warm-up
+        p.execute_checked((din.data_ptr(), din.numel() * 4), (dout.data_ptr(), dout.numel() * 4))
+    torch.cuda.synchronize()
+    lat_plain = []
+    t0 = time.perf_counter()
+    for i, (p, hi, ho) in enumerate(zip(plans, ins, outs)):
+        while time.perf_counter() - t0 < arrivals[i]:
+            pass
+        din[:hi.numel()].copy_(hi, non_blocking=True)
+        p.execute_checked((din.data_ptr(), din.numel() * 4), (dout.data_ptr(), dout.numel() * 4))
+        ho.copy_(dout[:ho.numel()], non_blocking=True)
+        torch.cuda.synchronize()
+        lat_plain.append(time.perf_counter() - t0 - arrivals[i])
+    plain_span = time.perf_counter() - t0 - arrivals[0]
+    del plans
+    # served path (plans become resident during a first unmeasured pass)
+    srv = w.FftServer(device=local, streams=4)
+    warm = [srv.submit(c, k, hi, ho) for c, k, hi, ho in zip(cfgs, kinds, ins, outs)]
+    for r in warm:
+        srv.wait(r, 600.0)
+    srv.reset_stats()
+    ids = [None] * len(reqs)
+
+    def feeder():
+        t1 = time.perf_counter()
+        for i in range(len(reqs)):
+            while time.perf_counter() - t1 < arrivals[i]:
+                pass
+            ids[i] = srv.submit(cfgs[i], kinds[i], ins[i], outs[i])
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    srv.drain(600.0)
+    st = srv.stats()
+    for r in ids:
+        srv.wait(r, 60.0)
+    srv.close()
+    lp = sorted(lat_plain)
+    plain = {"ffts_per_s": transforms / plain_span, "requests_per_s": len(reqs) / plain_span,
+             "p50_ms": lp[len(lp) // 2] * 1e3, "p99_ms": lp[int(len(lp) * 0.99)] * 1e3}
+    served = {"ffts_per_s": st["ffts_per_s"], "requests_per_s": st["requests_per_s"],
+              "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "groups": st["groups"],
+              "coalesced_requests": st["coalesced_requests"]}
+    return {"requests": len(reqs), "offered_rate_per_s": rate, "transforms": transforms,
+            "max_request_bytes": max_bytes, "served": served, "plain_per_request": plain,
+            "served_vs_plain_ffts": served["ffts_per_s"] / max(plain["ffts_per_s"], 1e-9)}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's CPU path (the planned CPU port of
     CpuFftPlan; the reference's Rust crate cannot be built here) on the host
@@ -200,6 +282,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -384,6 +467,13 @@ def main():
         except Exception as exc:
             cpu = {"error": str(exc)}
 
+    serving = None
+    if not args.no_serve:
+        try:
+            serving = serving_measurement(local)
+        except Exception as exc:
+            serving = {"error": str(exc)}
+
     lat = sorted(per_step)
     if rank == 0:
         out = {
@@ -402,6 +492,7 @@ def main():
                                                                         int(len(lat) * 0.99))],
                         "unit": "ms per 20,000-line batch"},
             "plain_per_plan": plain,
+            "serving": serving,
             "served_vs_plain": (value / world / plain["value"]) if plain else None,
             "gflops": world * sum(W.fft_flops(int(n)) for n in lengths) * args.steps
             / (total_ms / 1e3) / 1e9,

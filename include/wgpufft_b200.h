@@ -208,6 +208,33 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const v
 /* Task and launch summary as JSON (same length convention as the plan's). */
 b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_t* len);
 
+/* -------------------------------------------------------------- serving */
+
+/* Serving loop (no counterpart in the crate): a scheduler thread that keeps
+ * plans, tables and workspaces resident, admits requests by an HBM budget,
+ * coalesces queued requests of the same configuration into one batched
+ * execution (continuous batching: arrivals join the next group while
+ * earlier ones run), and overlaps groups on `nstreams` streams.  Requests
+ * carry host buffers (pinned memory lets the copies overlap); results are
+ * written back to host_out.  hbm_budget_bytes 0 = 120 GB. */
+typedef struct b2f_server b2f_server;
+b2f_status b2f_server_new(b2f_server** out, int32_t device, uint64_t hbm_budget_bytes,
+                          int32_t nstreams, int32_t coalesce);
+void b2f_server_free(b2f_server* server);
+/* Queues one transform (kind B2F_C2C / B2F_R2C / B2F_C2R of `cfg`). */
+b2f_status b2f_server_submit(b2f_server* server, const b2f_config* cfg, int32_t kind,
+                             const void* host_in, uint64_t in_bytes, void* host_out,
+                             uint64_t out_bytes, uint64_t* request_id);
+/* Blocks until the request completed (or timeout_s passed; 0 = 1 hour). */
+b2f_status b2f_server_wait(b2f_server* server, uint64_t request_id, double timeout_s);
+/* Blocks until nothing is queued or in flight. */
+b2f_status b2f_server_drain(b2f_server* server, double timeout_s);
+/* Completed/failed counts, groups, coalesced requests, p50/p99 latency
+ * (submission to completion), requests/s and FFTs/s over the served span,
+ * HBM in use, resident plans; same length convention as the plan's. */
+b2f_status b2f_server_stats_json(b2f_server* server, char* buf, uint64_t* len);
+void b2f_server_reset_stats(b2f_server* server);
+
 /* ---------------------------------------------------- allocation-free */
 
 /* No counterpart in the crate.  For callers that cannot allocate device

@@ -1,0 +1,131 @@
+"""GPU tests of the serving loop (b2f_server_*): every request's result is
+the same served in a mix (coalesced with other requests of its
+configuration, overlapped with other groups) as run alone through its own
+plan, within the f32 / f64 / df64 tolerances; admission refuses a request
+larger than the budget."""
+import numpy as np
+import pytest
+
+import wgpufft_b200 as w
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {w.FftPrecision.F32: 2e-6, w.FftPrecision.F64: 1e-14, w.FftPrecision.Df64: 1e-13}
+
+
+def host_arrays(cfg, kind, rng):
+    import torch
+    n = cfg.total_complex_len()
+    prec = cfg.precision()
+    packed = int(np.prod([cfg.shape()[0] // 2 + 1] + cfg.shape()[1:])) * cfg.batch()
+    if kind == w.FftTransformKind.R2c:
+        dt = np.float32 if prec == w.FftPrecision.F32 else np.float64
+        x = rng.uniform(-1, 1, n).astype(dt)
+        out_words = packed * 2
+    elif kind == w.FftTransformKind.C2r:
+        dt = np.float32 if prec == w.FftPrecision.F32 else np.float64
+        r = rng.uniform(-1, 1, n)
+        z = O.r2c_packed_f64(r, cfg.shape(), batch=cfg.batch())
+        x = z.astype(np.complex64 if dt == np.float32 else np.complex128).view(dt)
+        out_words = n
+    else:
+        z = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        if prec == w.FftPrecision.F32:
+            x, dt = z.astype(np.complex64).view(np.float32), np.float32
+        elif prec == w.FftPrecision.F64:
+            x, dt = z.view(np.float64), np.float64
+        else:
+            x, dt = O.df64_split(z), np.float32
+        out_words = x.size
+    hin = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+    hout = torch.zeros(out_words, dtype=hin.dtype).pin_memory()
+    return hin, hout
+
+
+def alone(cfg, kind, hin):
+    import torch
+    plan = {0: w.FftPlan.c2c, 1: w.FftPlan.r2c, 2: w.FftPlan.c2r}[int(kind)](cfg)
+    din = hin.cuda()
+    n_out = plan.required_output_buffer_size_bytes() // hin.element_size()
+    dout = torch.empty(n_out, dtype=hin.dtype, device="cuda")
+    plan.execute_checked(din, dout)
+    torch.cuda.synchronize()
+    return dout.cpu().numpy()
+
+
+def as_complex(a, prec):
+    if prec == w.FftPrecision.Df64:
+        return O.df64_join(a)
+    if a.dtype == np.float32:
+        return a.view(np.complex64).astype(np.complex128) if a.size % 2 == 0 else a.astype(np.complex128)
+    return a.view(np.complex128) if a.size % 2 == 0 else a.astype(np.complex128)
+
+
+def test_served_mix_equals_alone(cuda):
+    rng = np.random.default_rng(1)
+    F32, F64, DF = w.FftPrecision.F32, w.FftPrecision.F64, w.FftPrecision.Df64
+    C2C, R2C, C2R = w.FftTransformKind.C2c, w.FftTransformKind.R2c, w.FftTransformKind.C2r
+    kinds = [
+        (w.FftConfig.new(1024).with_batch(3), C2C),
+        (w.FftConfig.new(1024).with_batch(3), C2C),
+        (w.FftConfig.new(1024).with_batch(5), C2C),
+        (w.FftConfig.inverse(4099).with_batch(2), C2C),
+        (w.FftConfig.new_nd([64, 128]).with_batch(2), C2C),
+        (w.FftConfig.new_nd([64, 64, 64]), R2C),
+        (w.FftConfig.inverse_nd([64, 64, 64]), C2R),
+        (w.FftConfig.new(1 << 16).with_batch(2).with_precision(F64), C2C),
+        (w.FftConfig.new(3000).with_batch(4).with_precision(DF), C2C),
+        (w.FftConfig.new(1009).with_batch(7), C2C),
+        (w.FftConfig.new(1009).with_batch(7), C2C),
+    ]
+    srv = w.FftServer(streams=3)
+    reqs = []
+    for cfg, kind in kinds * 3:
+        hin, hout = host_arrays(cfg, kind, rng)
+        rid = srv.submit(cfg, kind, hin, hout)
+        reqs.append((cfg, kind, hin, hout, rid))
+    for cfg, kind, hin, hout, rid in reqs:
+        srv.wait(rid, 60.0)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    for cfg, kind, hin, hout, rid in reqs:
+        ref = alone(cfg, kind, hin)
+        got = hout.numpy()
+        prec = cfg.precision()
+        err = O.rel_l2(as_complex(got, prec), as_complex(ref, prec))
+        assert err <= TOL[prec], (cfg.shape(), kind, err)
+    srv.close()
+
+
+def test_served_results_match_oracle(cuda):
+    rng = np.random.default_rng(2)
+    srv = w.FftServer(streams=2)
+    cfg = w.FftConfig.new(2048).with_batch(4)
+    ins, outs, ids = [], [], []
+    for _ in range(8):
+        hin, hout = host_arrays(cfg, w.FftTransformKind.C2c, rng)
+        ids.append(srv.submit(cfg, w.FftTransformKind.C2c, hin, hout))
+        ins.append(hin)
+        outs.append(hout)
+    srv.drain(60.0)
+    for i, hin, hout in zip(ids, ins, outs):
+        srv.wait(i, 10.0)
+        x = hin.numpy().view(np.complex64).astype(np.complex128)
+        ref = O.c2c_nd_f64(x, [2048], batch=4)
+        assert O.rel_l2(hout.numpy().view(np.complex64), ref) < 2e-6
+    assert srv.stats()["coalesced_requests"] > 0
+    srv.close()
+
+
+def test_admission_refuses_oversized_request(cuda):
+    import torch
+    srv = w.FftServer(hbm_budget_bytes=1 << 20)
+    big = w.FftConfig.new(1 << 17)  # 1 MB in + 1 MB out > the 1 MB budget
+    hin2 = torch.zeros(2 << 17, dtype=torch.float32).pin_memory()
+    hout2 = torch.zeros(2 << 17, dtype=torch.float32).pin_memory()
+    rid = srv.submit(big, w.FftTransformKind.C2c, hin2, hout2)
+    with pytest.raises(w.FftError) as e:
+        srv.wait(rid, 30.0)
+    assert e.value.kind == "GpuPlanResourceAllocationFailed"
+    srv.close()

@@ -27,7 +27,8 @@ from typing import Iterable, Optional, Sequence, Tuple, Union
 
 __all__ = [
     "FftDirection", "Normalization", "FftPrecision", "FftTransformKind", "FftTuning",
-    "FftConfig", "FftPlan", "FftRecorder", "FftBatch", "FftError", "lib", "library_path",
+    "FftConfig", "FftPlan", "FftRecorder", "FftBatch", "FftServer", "FftError", "lib",
+    "library_path",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -97,6 +98,13 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_batch_execute": (st, [vp, vp, vp, u64, vp, u64]),
         "b2f_batch_diagnostics_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
         "b2f_batch_execute_parts": (st, [vp, vp, vp, u64, vp, u64, u32, i32]),
+        "b2f_server_new": (st, [pvp, i32, u64, i32, i32]),
+        "b2f_server_free": (None, [vp]),
+        "b2f_server_submit": (st, [vp, vp, i32, vp, u64, vp, u64, ctypes.POINTER(u64)]),
+        "b2f_server_wait": (st, [vp, u64, ctypes.c_double]),
+        "b2f_server_drain": (st, [vp, ctypes.c_double]),
+        "b2f_server_stats_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_server_reset_stats": (None, [vp]),
         "b2f_status_string": (ctypes.c_char_p, [st]),
         "b2f_last_error_message": (u64, [ctypes.c_char_p, u64]),
         "b2f_version": (ctypes.c_char_p, []),
@@ -567,6 +575,72 @@ class FftBatch:
                 self._ptr = None
         except Exception:
             pass
+
+
+class FftServer:
+    """Serving loop (b2f_server_*): resident plans, HBM-budget admission,
+    continuous batching of same-configuration requests, several streams."""
+
+    def __init__(self, device: Optional[int] = None, hbm_budget_bytes: int = 0, streams: int = 4,
+                 coalesce: bool = True):
+        self._ptr = ctypes.c_void_p()
+        _check(lib().b2f_server_new(ctypes.byref(self._ptr), -1 if device is None else int(device),
+                                    int(hbm_budget_bytes), int(streams), int(coalesce)))
+        self._keep = {}
+
+    def submit(self, config: FftConfig, kind: FftTransformKind, host_in, host_out) -> int:
+        """host_in/host_out: numpy arrays or pinned torch CPU tensors (kept
+        alive until the request is waited for)."""
+        ip, ib = _host_buf(host_in)
+        op, ob = _host_buf(host_out)
+        rid = ctypes.c_uint64()
+        with config._handle() as h:
+            _check(lib().b2f_server_submit(self._ptr, h.ptr, int(kind), ip, ib, op, ob,
+                                           ctypes.byref(rid)))
+        self._keep[rid.value] = (host_in, host_out)
+        return rid.value
+
+    def wait(self, request_id: int, timeout_s: float = 0.0) -> None:
+        try:
+            _check(lib().b2f_server_wait(self._ptr, request_id, timeout_s))
+        finally:
+            self._keep.pop(request_id, None)
+
+    def drain(self, timeout_s: float = 0.0) -> None:
+        _check(lib().b2f_server_drain(self._ptr, timeout_s))
+
+    def stats(self) -> dict:
+        n = ctypes.c_uint64(0)
+        _check(lib().b2f_server_stats_json(self._ptr, None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        n2 = ctypes.c_uint64(n.value + 1)
+        _check(lib().b2f_server_stats_json(self._ptr, buf, ctypes.byref(n2)))
+        return json.loads(buf.value.decode())
+
+    def reset_stats(self) -> None:
+        lib().b2f_server_reset_stats(self._ptr)
+
+    def close(self):
+        if self._ptr:
+            lib().b2f_server_free(self._ptr)
+            self._ptr = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _host_buf(b) -> Tuple[int, int]:
+    if isinstance(b, tuple):
+        return int(b[0]), int(b[1])
+    if hasattr(b, "data_ptr"):
+        return int(b.data_ptr()), int(b.numel() * b.element_size())
+    if hasattr(b, "ctypes"):
+        return int(b.ctypes.data), int(b.nbytes)
+    raise TypeError("host buffer must be a numpy array, a CPU tensor or (address, nbytes)")
 
 
 class FftRecorder:

@@ -6,9 +6,6 @@
 
 using namespace b2f;
 
-struct b2f_config {
-  Config cfg;
-};
 struct b2f_plan {
   Plan* plan;
 };

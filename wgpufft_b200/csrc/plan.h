@@ -128,3 +128,8 @@ const char* route_name(Route r);
 const char* axis_kind_name(AxisKind k);
 
 }  // namespace b2f
+
+// Opaque handles of the C ABI (shared by the translation units that use them).
+struct b2f_config {
+  b2f::Config cfg;
+};

@@ -77,3 +77,34 @@ def normal_complex(n: int, seed: int) -> np.ndarray:
 def fft_flops(n: int) -> float:
     """The 5 N log2 N convention for one complex transform of length N."""
     return 5.0 * n * math.log2(n) if n > 1 else 0.0
+
+
+def serving_requests(count: int, seed: int = 9, max_bytes: int = 64 << 20):
+    """Requests of the serving configuration: C2C or R2C, forward or inverse;
+    1D length log-uniform in [64, 2^22], 2D sides from {64, ..., 4096} or 3D
+    cubes from {32, 64, 128, 256}; batch uniform in 1..64; precision 80% f32,
+    10% f64, 10% df64 (df64 is C2C only, like the reference).  The batch is
+    reduced until one request holds at most max_bytes of input."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        r = rng.uniform()
+        if r < 1 / 3:
+            shape = [int(round(math.exp(rng.uniform(math.log(64), math.log(1 << 22)))))]
+        elif r < 2 / 3:
+            shape = [int(rng.choice([64, 128, 256, 512, 1024, 2048, 4096])) for _ in range(2)]
+        else:
+            c = int(rng.choice([32, 64, 128, 256]))
+            shape = [c, c, c]
+        batch = int(rng.integers(1, 65))
+        u = rng.uniform()
+        prec = 0 if u < 0.8 else (1 if u < 0.9 else 2)
+        real = rng.uniform() < 0.5 and prec != 2
+        inverse = rng.uniform() < 0.5
+        kind = (2 if inverse else 1) if real else 0
+        bpc = 8 if prec == 0 else 16
+        while batch > 1 and int(np.prod(shape)) * batch * bpc > max_bytes:
+            batch //= 2
+        out.append({"kind": kind, "shape": shape, "batch": batch, "precision": prec,
+                    "inverse": inverse})
+    return out
