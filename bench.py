@@ -10,9 +10,12 @@ flush is needed between steps).  One step = one batched launch over all
     execute_checked per line (what a caller of the reference's plan API does);
   - e2e: the batched step through the public API with the input copied from
     pinned host memory and the output copied back inside the timed region;
-  - roofline: the cluster (long-line) kernel alone, achieved algorithmic
-    GB/s (16 B per complex point per transform) against the measured HBM
-    copy bandwidth;
+  - roofline: the persistent CTA-queue kernel (k_batch_cta, every line with
+    the default routing), achieved algorithmic GB/s (16 B per complex point
+    per transform) against the measured HBM copy bandwidth, with the DRAM
+    traffic of an ncu capture (profiles/) scaled to the full launch;
+  - serving: an open-loop Poisson request stream through the serving loop
+    against the plain per-request path (p50/p99 latency, FFTs/s);
   - cpu_baseline: the planned CPU FFT (oracle/cpu_port.c, a C restatement of
     the reference's CpuFftPlan structure) on a bounded sample of the lines.
 
@@ -283,6 +286,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--lines", type=int, default=0,
+                    help="use only the first K lines of the workload (profiling-sized cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -300,6 +305,8 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     lengths = W.mixed_lengths()
+    if args.lines:
+        lengths = lengths[:args.lines]
     offsets = W.packed_offsets(lengths)
     total = int(lengths.sum())
     x = W.normal_complex(total, 5)
@@ -339,57 +346,53 @@ def main():
     value = world * len(lengths) * args.steps / (total_ms / 1e3)
     clocks = clk.summary()
 
-    # ---- roofline: the cluster kernel (long lines: most of the bytes) alone
-    cl_lines = lengths[lengths > 0]
-    nd = diag
-    rf = None
+    # ---- roofline of the dominant kernel.  With the default routing every
+    # line runs in k_batch_cta (one launch per step, after a 16-byte memset
+    # of the queue counters); its duration is timed on the launching stream.
     hbm_peak, peak_kind = load_peaks()
+    nd = diag
+    cta_bytes = 16 * int(nd.get("cta_elements", 0))
+    cl_bytes = 16 * int(nd.get("cluster_elements", 0))
+    rf = None
     try:
-        cl_bytes = 0
-        # lines classified to clusters are the ones the planner reports; recompute
-        # their bytes by running the cluster part alone and timing it
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for _ in range(2):
-            batch.execute_parts(dx, dy, 2, sequential=True)
-        torch.cuda.synchronize()
-        a0.record(stream)
-        reps = max(3, args.steps // 2)
-        for _ in range(reps):
-            batch.execute_parts(dx, dy, 2, sequential=True)
-        a1.record(stream)
-        torch.cuda.synchronize()
-        cl_ms = a0.elapsed_time(a1) / reps
-        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(3, args.steps)
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for _ in range(2):
             batch.execute_parts(dx, dy, 1, sequential=True)
         torch.cuda.synchronize()
-        b0.record(stream)
+        k0.record(stream)
         for _ in range(reps):
             batch.execute_parts(dx, dy, 1, sequential=True)
-        b1.record(stream)
+        k1.record(stream)
         torch.cuda.synchronize()
-        cta_ms = b0.elapsed_time(b1) / reps
-        cl_lens = np.array(nd.get("cluster_line_lengths", []))
-        cl_elems = int(nd.get("cluster_elements", 0))
-        cta_elems = int(nd.get("cta_elements", 0))
-        cl_alg = 16 * cl_elems
-        cta_alg = 16 * cta_elems
-        ach_cl = cl_alg / (cl_ms / 1e3) / 1e9
-        ach_cta = cta_alg / (cta_ms / 1e3) / 1e9
-        rf = {"bound": "hbm", "kernel": "k_batch_cluster<8> (lines too long for one CTA)",
-              "achieved": ach_cl, "peak": hbm_peak, "unit": "GB/s", "frac": ach_cl / hbm_peak,
-              "peak_kind": peak_kind, "traffic": None,
-              "algorithmic_bytes_per_launch": cl_alg, "ms_per_launch": cl_ms,
-              "other_kernel": {"kernel": "k_batch_cta (lines that fit one CTA)",
-                               "achieved": ach_cta, "frac": ach_cta / hbm_peak,
-                               "algorithmic_bytes_per_launch": cta_alg,
-                               "ms_per_launch": cta_ms},
+        cta_ms = k0.elapsed_time(k1) / reps
+        ach = cta_bytes / (cta_ms / 1e3) / 1e9
+        rf = {"bound": "hbm", "kernel": "k_batch_cta", "achieved": ach, "peak": hbm_peak,
+              "unit": "GB/s", "frac": ach / hbm_peak, "peak_kind": peak_kind,
+              "traffic": None, "algorithmic_bytes_per_launch": cta_bytes,
+              "ms_per_launch": cta_ms,
               "whole_step": {"achieved": alg_bytes / (ms_per_step / 1e3) / 1e9,
                              "frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}}
-        traffic_file = os.path.join(ROOT, "profiles", "batch_traffic.json")
-        if os.path.exists(traffic_file):
+        if cl_bytes:
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            batch.execute_parts(dx, dy, 2, sequential=True)
+            torch.cuda.synchronize()
+            c0.record(stream)
+            for _ in range(reps):
+                batch.execute_parts(dx, dy, 2, sequential=True)
+            c1.record(stream)
+            torch.cuda.synchronize()
+            cl_ms = c0.elapsed_time(c1) / reps
+            rf["other_kernel"] = {"kernel": "k_batch_cluster", "ms_per_launch": cl_ms,
+                                  "achieved": cl_bytes / (cl_ms / 1e3) / 1e9}
+        traffic_file = os.path.join(ROOT, "profiles", "k_batch_cta_traffic.json")
+        if os.path.exists(traffic_file) and not args.lines:
             with open(traffic_file) as f:
-                rf["traffic"] = json.load(f).get("k_batch_cluster_bytes_per_launch")
+                t = json.load(f)
+            # DRAM bytes of one capture on a subset, scaled to the full launch by
+            # the algorithmic bytes (the traffic grows with the points processed)
+            rf["traffic"] = t["dram_bytes_per_launch"] * cta_bytes / t["algorithmic_bytes"]
+            rf["traffic_note"] = t.get("note")
     except Exception as exc:  # measurement must not hide the headline
         rf = {"bound": "hbm", "error": str(exc)}
 
@@ -501,7 +504,8 @@ def main():
             "cpu_baseline": cpu,
             "accuracy": acc,
             "clocks": clocks,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": args.steps * (int(diag.get("cta_launches", 1)) + int(diag["cluster_tasks"] > 0)
+                                          + int(diag.get("cluster16_tasks", 0) > 0)),
             "batch": diag,
         }
         print(json.dumps(out), flush=True)

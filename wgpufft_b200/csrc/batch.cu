@@ -90,6 +90,8 @@ struct BatchPlan {
   unsigned int* d_counters = nullptr;  // [0] CTA queue, [1] cluster queue
   std::vector<void*> tables;
   uint32_t n_cta = 0, n_cl = 0, n_big = 0;
+  uint32_t phase_first[4] = {0, 0, 0, 0}, phase_count[4] = {0, 0, 0, 0};  // CTA-queue launches
+  uint64_t* d_line_scratch = nullptr;
   unsigned grid_big = 0;
   uint32_t buf_cta = 0, buf_cl = 0;
   size_t smem_cta = 0, smem_cl = 0;
@@ -117,6 +119,7 @@ struct BatchPlan {
     cudaFree(d_counters);
     cudaFree(d_scratch);
     cudaFree(d_tw);
+    cudaFree(d_line_scratch);
     if (side) cudaStreamDestroy(side);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
@@ -136,6 +139,26 @@ struct LenInfo {
   double cost = 0;
 };
 
+static bool pow2u(uint64_t v) { return v && !(v & (v - 1)); }
+
+// Line groups of the two passes of a long line: power-of-two passes run the
+// register path with 2048 points per group (128 threads with 16 values
+// each); other passes the shared-memory engine with 8 (or fewer) lines.
+static void set_long_groups(BatchLen& d) {
+  auto lg_of = [](uint32_t n, bool reg) -> uint32_t {
+    if (reg) {
+      uint32_t g = 2048 / n, l = 0;
+      while ((1u << (l + 1)) <= g) ++l;
+      return l;
+    }
+    return n <= 128 ? 4 : (n <= 256 ? 3 : 2);
+  };
+  d.reg1 = pow2u(d.N1) && d.N1 >= 16 && d.N1 <= 512;
+  d.reg2 = pow2u(d.N2) && d.N2 >= 16 && d.N2 <= 512;
+  d.lg = lg_of(d.N1, d.reg1);
+  d.lg2 = lg_of(d.N2, d.reg2);
+}
+
 // Chooses the execution of one distinct length.
 static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_t cta_cap,
                      size_t cl_cap, bool clusters, LenInfo& li) {
@@ -153,14 +176,17 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   const auto cta_bytes = [](uint64_t lbuf) { return 2 * (size_t)ld_f32(lbuf) * 8; };
   // long lines run as two passes of T = N1 * N2 (both <= 512) inside one
   // CTA; the most balanced split of T, 0 when none exists
+  // (power-of-two factors, which take the register path, count double)
   const auto split = [](uint64_t Tl) -> uint64_t {
     uint64_t best_a = 0;
     double best = 1e300;
     for (uint64_t a = 2; a <= 512; ++a) {
       if (Tl % a || Tl / a > 512 || Tl / a < 2) continue;
-      const double bal = std::fabs(std::log((double)a) - std::log((double)(Tl / a)));
-      if (bal < best) {
-        best = bal;
+      const uint64_t b2 = Tl / a;
+      double score = std::fabs(std::log((double)a) - std::log((double)b2));
+      score -= 4.0 * ((pow2u(a) && a >= 16) + (pow2u(b2) && b2 >= 16));
+      if (score < best) {
+        best = score;
         best_a = a;
       }
     }
@@ -200,7 +226,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     d.LD1 = ld_f32(d.N1);
     d.LD2 = ld_f32(d.N2);
     d.LD = std::max(d.LD1, d.LD2);
-    d.lg = std::max(d.N1, d.N2) <= 256 ? 3 : 2;
+    set_long_groups(d);
     d.sch = schedule_for(d.N1);
     d.sch2 = schedule_for(d.N2);
   } else if (is_prime_u64(N) && N >= 3 && is_smooth13(N - 1) && cta_bytes(N) <= cta_cap) {
@@ -231,8 +257,10 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     while (!smooth7(M)) ++M;
     uint64_t mlong = 0, a = 0;
     if (cta_bytes(M) > cta_cap && !clusters) {
-      // smallest 7-smooth convolution length that splits into two factors <= 512
-      for (uint64_t m = 2 * N - 1; m <= 262144; ++m) {
+      // the smallest 7-smooth convolution length that splits into factors <= 512
+      // (a power-of-two length would put both passes on the register path,
+      // but its extra points cost more than the register path saves)
+      for (uint64_t m = 2 * N - 1; !mlong && m <= 262144; ++m) {
         if (!smooth7(m)) continue;
         a = split(m);
         if (a) {
@@ -255,7 +283,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
       d.LD1 = ld_f32(d.N1);
       d.LD2 = ld_f32(d.N2);
       d.LD = std::max(d.LD1, d.LD2);
-      d.lg = std::max(d.N1, d.N2) <= 256 ? 3 : 2;
+      set_long_groups(d);
       d.sch = schedule_for(d.N1);
       d.sch2 = schedule_for(d.N2);
     } else {
@@ -442,14 +470,51 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   std::vector<uint64_t> sorted_off;
   std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks;
   std::vector<double> cta_cost, cl_cost, big_cost;
+  (void)0;
   std::vector<uint32_t> order_len(lens_list.size());
   for (size_t i = 0; i < lens_list.size(); ++i) order_len[i] = (uint32_t)i;
-  // lines sorted by length index; tasks reference contiguous runs
+  // lines sorted by length index; tasks reference contiguous runs.  Long
+  // lines become phase tasks: one task per column or row group, phase 1
+  // (with the short tasks) then 2, 3, 4 in later launches.
+  std::vector<BatchTask> phase_tasks[4];
+  std::vector<uint64_t> line_scratch;
+  uint64_t scratch_total = 0;
   for (size_t li = 0; li < lens_list.size(); ++li) {
     const auto& lines = by_len[lens_list[li]];
     const BatchLen& d = infos[li].d;
     bp->kind_lines[d.kind] += lines.size();
     const bool cl = d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE;
+    const bool lng = d.kind == BK_LONG || d.kind == BK_LONG_BLUE;
+    if (lng) {
+      const int nph = d.kind == BK_LONG_BLUE ? 4 : 2;
+      for (uint64_t line : lines) {
+        const uint32_t idx = (uint32_t)sorted_off.size();
+        sorted_off.push_back(offsets[line]);
+        line_scratch.resize(idx + 1, 0);
+        line_scratch[idx] = scratch_total;
+        scratch_total += (d.kind == BK_LONG_BLUE ? 2ull : 1ull) * d.M;
+        bp->elems_cta += lens_list[li];
+        bp->lines_cta += 1;
+        for (int ph = 1; ph <= nph; ++ph) {
+          const uint32_t extent = (ph % 2 == 1) ? d.N2 : d.N1;  // column passes walk N2
+          const uint32_t Gp = (ph % 2 == 1) ? (1u << d.lg) : (1u << d.lg2);
+          for (uint32_t g0 = 0; g0 < extent; g0 += Gp) {
+            BatchTask t;
+            t.len = (uint32_t)li;
+            t.first = idx;
+            t.count = g0;
+            t.pad = (uint32_t)ph;
+            if (ph == 1) {
+              cta_tasks.push_back(t);
+              cta_cost.push_back((double)Gp * (ph % 2 == 1 ? d.N1 : d.N2) * 8.0);
+            } else {
+              phase_tasks[ph - 1].push_back(t);
+            }
+          }
+        }
+      }
+      continue;
+    }
     for (size_t s = 0; s < lines.size(); s += (cl ? 1 : d.G)) {
       BatchTask t;
       t.len = (uint32_t)li;
@@ -457,6 +522,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       t.count = (uint32_t)std::min<size_t>(cl ? 1 : d.G, lines.size() - s);
       t.pad = 0;
       for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[lines[s + c]]);
+      line_scratch.resize(sorted_off.size(), 0);
       if (cl && d.P == kClusterBig) {
         big_tasks.push_back(t);
         big_cost.push_back(infos[li].cost);
@@ -496,7 +562,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     const BatchLen& d = li.d;
     if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) buf_cl = std::max(buf_cl, d.LD);
     else if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE)
-      buf_cta = std::max<uint32_t>(buf_cta, (1u << d.lg) * d.LD);
+      buf_cta = std::max<uint32_t>(buf_cta, std::max((1u << d.lg) * d.LD1, (1u << d.lg2) * d.LD2));
     else buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
     if (d.kind == BK_LONG) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, d.N);
     if (d.kind == BK_LONG_BLUE) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, 2ull * d.M);
@@ -509,16 +575,28 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   std::vector<BatchLen> dl(infos.size());
   for (size_t i = 0; i < infos.size(); ++i) dl[i] = infos[i].d;
   std::vector<BatchTask> all = cta_tasks;
+  bp->phase_first[0] = 0;
+  bp->phase_count[0] = (uint32_t)cta_tasks.size();
+  for (int ph = 1; ph < 4; ++ph) {
+    bp->phase_first[ph] = (uint32_t)all.size();
+    bp->phase_count[ph] = (uint32_t)phase_tasks[ph].size();
+    all.insert(all.end(), phase_tasks[ph].begin(), phase_tasks[ph].end());
+  }
+  bp->n_cta = (uint32_t)all.size();
   all.insert(all.end(), cl_tasks.begin(), cl_tasks.end());
   all.insert(all.end(), big_tasks.begin(), big_tasks.end());
   bool okc = cudaMalloc(&bp->d_lens, dl.size() * sizeof(BatchLen)) == cudaSuccess &&
              cudaMalloc(&bp->d_tasks, std::max<size_t>(1, all.size()) * sizeof(BatchTask)) == cudaSuccess &&
              cudaMalloc(&bp->d_off, sorted_off.size() * 8) == cudaSuccess &&
-             cudaMalloc(&bp->d_counters, 4 * sizeof(unsigned int)) == cudaSuccess;
+             cudaMalloc(&bp->d_counters, 8 * sizeof(unsigned int)) == cudaSuccess;
   if (!okc) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
   cudaMemcpy(bp->d_lens, dl.data(), dl.size() * sizeof(BatchLen), cudaMemcpyHostToDevice);
   if (!all.empty()) cudaMemcpy(bp->d_tasks, all.data(), all.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
   cudaMemcpy(bp->d_off, sorted_off.data(), sorted_off.size() * 8, cudaMemcpyHostToDevice);
+  line_scratch.resize(sorted_off.size(), 0);
+  if (cudaMalloc(&bp->d_line_scratch, line_scratch.size() * 8) != cudaSuccess)
+    return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
+  cudaMemcpy(bp->d_line_scratch, line_scratch.data(), line_scratch.size() * 8, cudaMemcpyHostToDevice);
   // launch shapes
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
@@ -528,9 +606,11 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cta, kCtaThreads, bp->smem_cta);
     per_sm = std::max(per_sm, 1);
-    bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, bp->n_cta);
-    if (bp->slot_elems) {
-      bp->scratch_bytes = (uint64_t)bp->grid_cta * bp->slot_elems * 8;
+    uint32_t most = 0;
+    for (int ph = 0; ph < 4; ++ph) most = std::max(most, bp->phase_count[ph]);
+    bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, std::max<uint32_t>(most, 1));
+    if (scratch_total) {
+      bp->scratch_bytes = scratch_total * 8;
       if (cudaMalloc(&bp->d_scratch, bp->scratch_bytes) != cudaSuccess)
         return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch scratch allocation failed");
     }
@@ -590,7 +670,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   os << "{\"lines\":" << nlines << ",\"distinct_lengths\":" << bp->distinct
      << ",\"cta_lines\":" << bp->lines_cta << ",\"cluster_lines\":" << bp->lines_cl
      << ",\"cta_elements\":" << bp->elems_cta << ",\"cluster_elements\":" << bp->elems_cl
-     << ",\"cta_tasks\":" << bp->n_cta << ",\"cluster_tasks\":" << bp->n_cl
+     << ",\"cta_tasks\":" << bp->n_cta << ",\"cta_launches\":"
+     << ((bp->phase_count[0] > 0) + (bp->phase_count[1] > 0) + (bp->phase_count[2] > 0) + (bp->phase_count[3] > 0)) << ",\"cluster_tasks\":" << bp->n_cl
      << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
      << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
      << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5]
@@ -613,7 +694,7 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != bp.device) cudaSetDevice(bp.device);
-  cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, 4 * sizeof(unsigned int), st);
+  cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, 8 * sizeof(unsigned int), st);
   BatchParams p{};
   p.in = (const c32*)in;
   p.out = (c32*)out;
@@ -621,6 +702,7 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
   p.line_off = bp.d_off;
   p.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
   p.scratch = bp.d_scratch;
+  p.line_scratch = bp.d_line_scratch;
   p.tw = bp.d_tw;
   p.slot_elems = bp.slot_elems;
   const bool run_cl = (bp.n_cl || bp.n_big) && (parts & 2);
@@ -660,12 +742,15 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
     }
   }
   if (e == cudaSuccess && run_cta) {
-    BatchParams pt = p;
-    pt.tasks = bp.d_tasks;
-    pt.ntasks = bp.n_cta;
-    pt.counter = bp.d_counters;
-    k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
-    e = cudaGetLastError();
+    for (int ph = 0; ph < 4 && e == cudaSuccess; ++ph) {
+      if (bp.phase_count[ph] == 0) continue;
+      BatchParams pt = p;
+      pt.tasks = bp.d_tasks + bp.phase_first[ph];
+      pt.ntasks = bp.phase_count[ph];
+      pt.counter = bp.d_counters + 4 + ph;
+      k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+      e = cudaGetLastError();
+    }
   }
   if (e == cudaSuccess && run_cl && !sequential) {
     e = cudaEventRecord(bp.join, bp.side);

@@ -22,6 +22,7 @@
 #include <cooperative_groups.h>
 
 #include "kernels_impl.cuh"
+#include "regfft.cuh"
 
 namespace b2f {
 
@@ -54,7 +55,9 @@ struct BatchLen {
   //   BK_LONG: T = N, B = N2 (a < N1);  cluster kinds: T = M, B = L (a < P).
   uint32_t ta, tb;
   FastDiv dB;
-  uint32_t lg;    // long kinds: log2 of the lines per pass group (G = 1 << lg)
+  uint32_t lg;    // long kinds: log2 of the lines per column-pass group (G = 1 << lg)
+  uint32_t lg2;   // long kinds: log2 of the lines per row-pass group
+  uint32_t reg1, reg2;  // the column / row pass length is a power of two: register path
   Schedule sch;   // schedule of the per-CTA FFT length (N, p-1, M, L or N1)
   Schedule sch2;  // BK_LONG: schedule of N2
 };
@@ -71,6 +74,7 @@ struct BatchParams {
   c32* out;
   c32* scratch;          // BK_LONG: one slot of slot_elems per CTA
   uint64_t slot_elems;
+  const uint64_t* line_scratch;  // phased long lines: scratch offset of each line
   const c32* tw;         // stage and inter-pass twiddle tables (FP64-built, rounded once)
   const BatchLen* lens;
   const BatchTask* tasks;
@@ -98,6 +102,34 @@ FFT_D void copy_words(T* dst, const T* src, uint32_t tid, uint32_t nthreads) {
   const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
   uint32_t* d = reinterpret_cast<uint32_t*>(dst);
   for (uint32_t i = tid; i < sizeof(T) / 4; i += nthreads) d[i] = s[i];
+}
+
+// Register-resident FFT of G power-of-two lines of N (16..512) already in
+// shared memory (line c at sm[c*LD + pidx(n)]), transformed in place and
+// left in natural order: each of the G*N/16 active threads keeps 16 values
+// in registers through the radix-16 stages (regfft.cuh), shared memory is
+// only the exchange between stages.  Ends with a barrier.
+FFT_D void reg_fft_group_smem(c32* sm, uint32_t G, uint32_t N, uint32_t LD, uint32_t tid,
+                              const Schedule& sch, const c32* __restrict__ tw) {
+  constexpr int PAD = PadOf<float>::value;
+  constexpr int E = 16;
+  const uint32_t TL = N / E;
+  const uint32_t c = tid / TL, t = tid - c * TL;
+  const bool valid = c < G;
+  c32* line = sm + (valid ? c : 0) * LD;
+  c32 v[E];
+  const uint32_t last = sch.nst - 1;
+  for (uint32_t s = 0;; ++s) {
+    const StageDesc& sd = sch.st[s];
+    if (valid) {
+      reg_read_any<float, E, PAD>(sd.R, v, line, t, TL, sd.NR);
+      reg_compute_any<float, E, PAD>(sd.R, v, t, TL, sd.Ns, tw, sd.tw_off);
+    }
+    __syncthreads();
+    if (valid) reg_write_any<float, E, PAD>(sd.R, v, line, t, TL, sd.Ns);
+    __syncthreads();
+    if (s == last) break;
+  }
 }
 
 // W_T^j from the two-level table: j = a*B + b.
@@ -235,96 +267,141 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
 enum LongIn : uint32_t { LI_X = 0, LI_X_CHIRP = 1, LI_SLOT = 2 };
 enum LongOut : uint32_t { LO_X = 0, LO_SLOT_SPECTRUM = 1, LO_X_CHIRP = 2 };
 
-FFT_D void long_column_pass(const BatchParams& bp, const BatchLen& L, int64_t base,
-                            const c32* src_slot, c32* dst, LongIn mode, c32* A, c32* B,
-                            uint32_t tid, uint32_t T) {
+FFT_D void long_column_group(const BatchParams& bp, const BatchLen& L, int64_t base,
+                             const c32* src_slot, c32* dst, LongIn mode, uint32_t c0, c32* A,
+                             c32* B, uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<float>::value;
   const uint32_t N = L.N, N1 = L.N1, N2 = L.N2, lg = L.lg, G = 1u << lg;
   const bool inv = bp.inverse;
-  for (uint32_t c0 = 0; c0 < N2; c0 += G) {
+  for (uint32_t e = tid; e < (N1 << lg); e += T) {
+    const uint32_t n1 = e >> lg, c = e & (G - 1);
+    c32* d = &A[c * L.LD1 + pidx<PAD>(n1)];
+    const uint32_t n = N2 * n1 + c0 + c;
+    if (c0 + c >= N2) {
+      *d = czero<float>();
+    } else if (mode == LI_SLOT) {
+      cp_async8(d, &src_slot[n]);
+    } else if (mode == LI_X) {
+      cp_async8(d, &bp.in[base + n]);
+    } else {  // chirped, zero beyond the line
+      if (n < N) {
+        c32 v = bp.in[base + n];
+        if (inv) v.im = -v.im;
+        *d = cmul(v, chirp<float>(n, N));
+      } else {
+        *d = czero<float>();
+      }
+    }
+  }
+  cp_async_wait_all();
+  if (inv && mode == LI_X) {
     for (uint32_t e = tid; e < (N1 << lg); e += T) {
       const uint32_t n1 = e >> lg, c = e & (G - 1);
-      c32* d = &A[c * L.LD1 + pidx<PAD>(n1)];
-      const uint32_t n = N2 * n1 + c0 + c;
-      if (c0 + c >= N2) {
-        *d = czero<float>();
-      } else if (mode == LI_SLOT) {
-        cp_async8(d, &src_slot[n]);
-      } else if (mode == LI_X) {
-        cp_async8(d, &bp.in[base + n]);
-      } else {  // chirped, zero beyond the line
-        if (n < N) {
-          c32 v = bp.in[base + n];
-          if (inv) v.im = -v.im;
-          *d = cmul(v, chirp<float>(n, N));
-        } else {
-          *d = czero<float>();
-        }
-      }
+      c32& v = A[c * L.LD1 + pidx<PAD>(n1)];
+      v.im = -v.im;
     }
-    cp_async_wait_all();
-    if (inv && mode == LI_X) {
-      for (uint32_t e = tid; e < (N1 << lg); e += T) {
-        const uint32_t n1 = e >> lg, c = e & (G - 1);
-        c32& v = A[c * L.LD1 + pidx<PAD>(n1)];
-        v.im = -v.im;
-      }
-    }
-    __syncthreads();
-    const c32* r = fft_lines_smem<float>(A, B, L.sch, G, L.LD1, tid, T, bp.tw);
-    for (uint32_t e = tid; e < (N1 << lg); e += T) {
-      const uint32_t k1 = e >> lg, c = e & (G - 1);
-      if (c0 + c < N2) {
-        c32 v = r[c * L.LD1 + pidx<PAD>(k1)];
-        v = cmul(v, tw2(bp, L, (c0 + c) * k1, N2));
-        dst[(uint64_t)N2 * k1 + c0 + c] = v;
-      }
-    }
-    __syncthreads();
   }
+  __syncthreads();
+  const c32* r;
+  if (L.reg1) {
+    reg_fft_group_smem(A, G, N1, L.LD1, tid, L.sch, bp.tw);
+    r = A;
+  } else {
+    r = fft_lines_smem<float>(A, B, L.sch, G, L.LD1, tid, T, bp.tw);
+  }
+  for (uint32_t e = tid; e < (N1 << lg); e += T) {
+    const uint32_t k1 = e >> lg, c = e & (G - 1);
+    if (c0 + c < N2) {
+      c32 v = r[c * L.LD1 + pidx<PAD>(k1)];
+      v = cmul(v, tw2(bp, L, (c0 + c) * k1, N2));
+      dst[(uint64_t)N2 * k1 + c0 + c] = v;
+    }
+  }
+  __syncthreads();
+}
+
+FFT_D void long_column_pass(const BatchParams& bp, const BatchLen& L, int64_t base,
+                            const c32* src_slot, c32* dst, LongIn mode, c32* A, c32* B,
+                            uint32_t tid, uint32_t T) {
+  for (uint32_t c0 = 0; c0 < L.N2; c0 += 1u << L.lg)
+    long_column_group(bp, L, base, src_slot, dst, mode, c0, A, B, tid, T);
+}
+
+FFT_D void long_row_group(const BatchParams& bp, const BatchLen& L, int64_t base, const c32* slot,
+                          c32* dst_slot, LongOut mode, uint32_t k0, c32* A, c32* B, uint32_t tid,
+                          uint32_t T) {
+  constexpr int PAD = PadOf<float>::value;
+  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2, lg = L.lg2, G = 1u << lg;
+  const bool inv = bp.inverse;
+  const float sc = L.scale;
+#pragma unroll 1
+  for (uint32_t rr = 0; rr < G; ++rr) {
+    const bool ok = k0 + rr < N1;
+    const c32* row = slot + (uint64_t)N2 * (k0 + rr);
+    for (uint32_t n2 = tid; n2 < N2; n2 += T) {
+      if (ok) cp_async8(&A[rr * L.LD2 + pidx<PAD>(n2)], &row[n2]);
+      else A[rr * L.LD2 + pidx<PAD>(n2)] = czero<float>();
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const c32* r;
+  if (L.reg2) {
+    reg_fft_group_smem(A, G, N2, L.LD2, tid, L.sch2, bp.tw);
+    r = A;
+  } else {
+    r = fft_lines_smem<float>(A, B, L.sch2, G, L.LD2, tid, T, bp.tw);
+  }
+  for (uint32_t e = tid; e < (N2 << lg); e += T) {
+    const uint32_t k2 = e >> lg, rr = e & (G - 1);
+    if (k0 + rr >= N1) continue;
+    const uint32_t k = k0 + rr + N1 * k2;
+    c32 v = r[rr * L.LD2 + pidx<PAD>(k2)];
+    if (mode == LO_X) {
+      v.re *= sc;
+      v.im = inv ? -v.im * sc : v.im * sc;
+      bp.out[base + k] = v;
+    } else if (mode == LO_SLOT_SPECTRUM) {
+      v = cmul(v, L.bhat[k]);
+      v.im = -v.im;  // conjugated: the next forward FFT computes the inverse
+      dst_slot[k] = v;
+    } else if (k < N) {
+      v.im = -v.im;
+      v = cmul(v, chirp<float>(k, N));
+      v.re *= sc;
+      v.im = inv ? -v.im * sc : v.im * sc;
+      bp.out[base + k] = v;
+    }
+  }
+  __syncthreads();
 }
 
 FFT_D void long_row_pass(const BatchParams& bp, const BatchLen& L, int64_t base, const c32* slot,
                          c32* dst_slot, LongOut mode, c32* A, c32* B, uint32_t tid, uint32_t T) {
-  constexpr int PAD = PadOf<float>::value;
-  const uint32_t N = L.N, N1 = L.N1, N2 = L.N2, lg = L.lg, G = 1u << lg;
-  const bool inv = bp.inverse;
-  const float sc = L.scale;
-  for (uint32_t k0 = 0; k0 < N1; k0 += G) {
-#pragma unroll 1
-    for (uint32_t rr = 0; rr < G; ++rr) {
-      const bool ok = k0 + rr < N1;
-      const c32* row = slot + (uint64_t)N2 * (k0 + rr);
-      for (uint32_t n2 = tid; n2 < N2; n2 += T) {
-        if (ok) cp_async8(&A[rr * L.LD2 + pidx<PAD>(n2)], &row[n2]);
-        else A[rr * L.LD2 + pidx<PAD>(n2)] = czero<float>();
-      }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const c32* r = fft_lines_smem<float>(A, B, L.sch2, G, L.LD2, tid, T, bp.tw);
-    for (uint32_t e = tid; e < (N2 << lg); e += T) {
-      const uint32_t k2 = e >> lg, rr = e & (G - 1);
-      if (k0 + rr >= N1) continue;
-      const uint32_t k = k0 + rr + N1 * k2;
-      c32 v = r[rr * L.LD2 + pidx<PAD>(k2)];
-      if (mode == LO_X) {
-        v.re *= sc;
-        v.im = inv ? -v.im * sc : v.im * sc;
-        bp.out[base + k] = v;
-      } else if (mode == LO_SLOT_SPECTRUM) {
-        v = cmul(v, L.bhat[k]);
-        v.im = -v.im;  // conjugated: the next forward FFT computes the inverse
-        dst_slot[k] = v;
-      } else if (k < N) {
-        v.im = -v.im;
-        v = cmul(v, chirp<float>(k, N));
-        v.re *= sc;
-        v.im = inv ? -v.im * sc : v.im * sc;
-        bp.out[base + k] = v;
-      }
-    }
-    __syncthreads();
+  for (uint32_t k0 = 0; k0 < L.N1; k0 += 1u << L.lg2)
+    long_row_group(bp, L, base, slot, dst_slot, mode, k0, A, B, tid, T);
+}
+
+// One phase of a long line, one pass group per task (task.pad = phase,
+// task.count = first column / row of the group):
+//   smooth lines:    1 column pass x -> scratch, 2 row pass scratch -> out;
+//   Bluestein lines: 1 chirped column pass x -> s1, 2 row pass + spectrum
+//                    product s1 -> s2, 3 column pass s2 -> s1, 4 row pass
+//                    + chirp s1 -> out.
+// Consecutive phases are consecutive launches, so every task of a phase
+// sees the previous phase's scratch complete.
+FFT_D void long_phase_task(const BatchParams& bp, const BatchLen& L, int64_t base, c32* slot,
+                           uint32_t phase, uint32_t g0, c32* A, c32* B, uint32_t tid,
+                           uint32_t T) {
+  const bool blue = L.kind == BK_LONG_BLUE;
+  c32* s1 = slot;
+  c32* s2 = slot + L.M;
+  switch (phase) {
+    case 1: long_column_group(bp, L, base, nullptr, s1, blue ? LI_X_CHIRP : LI_X, g0, A, B, tid, T); break;
+    case 2: long_row_group(bp, L, base, s1, s2, blue ? LO_SLOT_SPECTRUM : LO_X, g0, A, B, tid, T); break;
+    case 3: long_column_group(bp, L, base, s2, s1, LI_SLOT, g0, A, B, tid, T); break;
+    case 4: long_row_group(bp, L, base, s1, nullptr, LO_X_CHIRP, g0, A, B, tid, T); break;
+    default: break;
   }
 }
 
@@ -356,6 +433,7 @@ __global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ Ba
   __shared__ BatchLen s_len;
   __shared__ int64_t s_base[kBatchMaxG];
   __shared__ uint32_t s_task;
+  uint32_t s_len_idx = 0xFFFFFFFFu;  // length descriptor currently in s_len (same in every thread)
   c32* A = reinterpret_cast<c32*>(smem_raw);
   c32* B = A + buf_elems;
   c32* x0s = B + buf_elems;
@@ -367,9 +445,17 @@ __global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ Ba
     const uint32_t t = s_task;
     if (t >= bp.ntasks) break;
     const BatchTask task = bp.tasks[t];
-    copy_words(&s_len, bp.lens + task.len, tid, T);
-    for (uint32_t c = tid; c < task.count; c += T) s_base[c] = (int64_t)bp.line_off[task.first + c];
+    if (task.len != s_len_idx) copy_words(&s_len, bp.lens + task.len, tid, T);
+    s_len_idx = task.len;
+    const uint32_t nbase = task.pad != 0 ? 1u : task.count;
+    for (uint32_t c = tid; c < nbase; c += T) s_base[c] = (int64_t)bp.line_off[task.first + c];
     __syncthreads();
+    if (task.pad != 0) {  // one phase group of a long line
+      long_phase_task(bp, s_len, s_base[0], bp.scratch + bp.line_scratch[task.first], task.pad,
+                      task.count, A, B, tid, T);
+      __syncthreads();
+      continue;
+    }
     switch (s_len.kind) {
       case BK_MIXED: batch_mixed(bp, s_len, s_base, task.count, A, B, tid, T); break;
       case BK_RADER: batch_rader(bp, s_len, s_base, task.count, A, B, x0s, X0s, tid, T); break;
