@@ -103,33 +103,9 @@ class ClockSampler:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def max_over_ranks(world, value: float) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from wgpufft_b200.replicas import Replicas
+    rep = Replicas()
+    return rep
 
 
 def cpu_sample_rate(lengths, offsets, x, seconds_target=10.0, threads=0):
@@ -250,6 +226,102 @@ def serving_measurement(local, count=300, rate=2000.0, max_bytes=8 << 20, seed=9
             "served_vs_plain_ffts": served["ffts_per_s"] / max(plain["ffts_per_s"], 1e-9)}
 
 
+def config_measurements(local, hbm_peak):
+    """Every BASELINE configuration through the plain per-plan path: ms per
+    transform (CUDA events, inputs resident, no copies), algorithmic GB/s
+    (16 B per complex point per f32 transform, 32 B for f64/df64; real
+    transforms 4 N_real + 8 N_packed), fraction of the measured HBM
+    bandwidth, and GFLOP/s (5 N log2 N per complex line, 2.5 N log2 N per
+    real one)."""
+    import math
+
+    import torch
+    import wgpufft_b200 as w
+
+    F32, F64, DF64 = w.FftPrecision.F32, w.FftPrecision.F64, w.FftPrecision.Df64
+    C2C, R2C, C2R = w.FftTransformKind.C2c, w.FftTransformKind.R2c, w.FftTransformKind.C2r
+    cases = [
+        ("1d_1024x512_c2c_f32", w.FftConfig.new(1024).with_batch(512), C2C, False, True),
+        ("2d_[2048,4096]_fwd+inv_in_place", w.FftConfig.new_nd([2048, 4096]), C2C, True, False),
+        ("2d_[4096,2048]_fwd+inv_in_place", w.FftConfig.new_nd([4096, 2048]), C2C, True, False),
+        ("3d_256^3_r2c", w.FftConfig.new_nd([256, 256, 256]), R2C, False, False),
+        ("3d_256^3_c2r", w.FftConfig.inverse_nd([256, 256, 256]), C2R, False, False),
+        ("1d_127x264208_rader", w.FftConfig.new(127).with_batch(264208), C2C, False, False),
+        ("1d_1009x33255", w.FftConfig.new(1009).with_batch(33255), C2C, False, False),
+        ("1d_4099x8186", w.FftConfig.new(4099).with_batch(8186), C2C, False, False),
+        ("1d_15015x2234", w.FftConfig.new(15015).with_batch(2234), C2C, False, False),
+        ("1d_2^20x32", w.FftConfig.new(1 << 20).with_batch(32), C2C, False, False),
+        ("1d_2^26", w.FftConfig.new(1 << 26), C2C, False, False),
+        ("1d_2^24", w.FftConfig.new(1 << 24), C2C, False, False),
+        ("2d_8192x8192", w.FftConfig.new_nd([8192, 8192]), C2C, False, False),
+        ("1d_2^20x16_f64", w.FftConfig.new(1 << 20).with_batch(16).with_precision(F64), C2C,
+         False, False),
+        ("1d_2^20x16_df64", w.FftConfig.new(1 << 20).with_batch(16).with_precision(DF64), C2C,
+         False, False),
+    ]
+    out = {}
+    stream = torch.cuda.current_stream()
+    for name, cfg, kind, pair, graph in cases:
+        try:
+            mk = {0: w.FftPlan.c2c, 1: w.FftPlan.r2c, 2: w.FftPlan.c2r}[int(kind)]
+            plan = mk(cfg, device=local)
+            inv = None
+            if pair:
+                inv = w.FftPlan.c2c(cfg.with_direction(w.FftDirection.Inverse), device=local)
+            ib, ob = plan.required_input_buffer_size_bytes(), plan.required_output_buffer_size_bytes()
+            a = torch.randn(max(ib, ob) // 4 + 4, device="cuda")
+            o = torch.empty(ob // 4 + 4, device="cuda")
+
+            def step():
+                if pair:
+                    plan.execute_in_place(a)
+                    inv.execute_in_place(a)
+                else:
+                    plan.execute_checked(a, o)
+            reps = 20
+            rec = None
+            if graph:
+                rec = w.FftRecorder()
+                for _ in range(100):
+                    plan.record(rec, a, o)
+                rec.finish()
+            for _ in range(3):
+                step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if rec is not None:
+                for _ in range(reps):
+                    rec.submit()
+            else:
+                for _ in range(reps):
+                    step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps / (100 if rec is not None else 1)
+            n_tr = 2 if pair else 1
+            total = cfg.total_complex_len()
+            if kind == C2C:
+                bpp = 16 if cfg.precision() == F32 else 32
+                alg = bpp * total * n_tr
+            else:
+                packed = int(np.prod([cfg.shape()[0] // 2 + 1] + cfg.shape()[1:])) * cfg.batch()
+                alg = 4 * total + 8 * packed
+            lines_flops = 0.0
+            logical = int(np.prod(cfg.shape()))
+            per = (2.5 if kind != C2C else 5.0) * logical * math.log2(logical) * cfg.batch()
+            gbs = alg / (ms / 1e3) / 1e9
+            out[name] = {"ms": ms, "GBps_alg": gbs, "frac_hbm": gbs / hbm_peak,
+                         "GFLOPs": n_tr * per / (ms / 1e3) / 1e9,
+                         "stages": [s["kind"] + ":" + s["label"] for s in plan.diagnostics()["stages"]],
+                         "timing": "CUDA graph of 100 executions" if rec is not None else "events"}
+            del plan, inv, a, o, rec
+            torch.cuda.empty_cache()
+        except Exception as exc:
+            out[name] = {"error": str(exc)}
+    return out
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's CPU path (the planned CPU port of
     CpuFftPlan; the reference's Rust crate cannot be built here) on the host
@@ -286,16 +358,23 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--lines", type=int, default=0,
                     help="use only the first K lines of the workload (profiling-sized cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    world, rank, local = dist_setup(args)
+    rep = dist_setup(args)
+    world, rank, local = rep.world, rep.rank, rep.local
+
+    def barrier(_world):
+        rep.barrier()
+
+    def max_over_ranks(_world, value):
+        return rep.max(value)
+
     if args.impl == "reference":
         run_reference(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        rep.close()
         return
 
     import torch
@@ -470,6 +549,10 @@ def main():
         except Exception as exc:
             cpu = {"error": str(exc)}
 
+    configs = None
+    if not args.no_configs and rank == 0:
+        configs = config_measurements(local, hbm_peak)
+
     serving = None
     if not args.no_serve:
         try:
@@ -496,6 +579,7 @@ def main():
                         "unit": "ms per 20,000-line batch"},
             "plain_per_plan": plain,
             "serving": serving,
+            "configs": configs,
             "served_vs_plain": (value / world / plain["value"]) if plain else None,
             "gflops": world * sum(W.fft_flops(int(n)) for n in lengths) * args.steps
             / (total_ms / 1e3) / 1e9,
@@ -509,10 +593,7 @@ def main():
             "batch": diag,
         }
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        barrier(world)
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
