@@ -187,7 +187,7 @@ b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_
 /* b2f_batch_new with flags: bit 0 (B2F_BATCH_CLUSTERS) runs lines too long
  * for one CTA on 8/16-CTA thread-block clusters that keep the whole line in
  * distributed shared memory (one HBM pass, fewer lines in flight) instead
- * of the default two-pass per-CTA route through L2-resident scratch. */
+ * of the default column and row passes through a scratch region. */
 #define B2F_BATCH_CLUSTERS 1u
 b2f_status b2f_batch_new_ex(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
                             uint64_t count, int32_t direction, int32_t normalization,
@@ -199,9 +199,9 @@ uint64_t b2f_batch_required_buffer_size_bytes(const b2f_batch* batch);
 b2f_status b2f_batch_execute(const b2f_batch* batch, void* stream, const void* in,
                              uint64_t in_bytes, void* out, uint64_t out_bytes);
 /* b2f_batch_execute restricted to a subset of the lines, for measuring one
- * kernel alone: parts bit 0 = lines that fit one CTA, bit 1 = cluster lines;
- * sequential != 0 runs both kernels on `stream` one after the other instead
- * of overlapping them on two streams. */
+ * kernel alone: parts bit 0 = lines that fit one CTA, bit 1 = cluster lines,
+ * bit 2 = the column/row passes of the other long lines; sequential != 0
+ * runs the cluster kernels on `stream` too instead of a second stream. */
 b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const void* in,
                                    uint64_t in_bytes, void* out, uint64_t out_bytes,
                                    uint32_t parts, int32_t sequential);

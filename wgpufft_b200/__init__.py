@@ -552,8 +552,8 @@ class FftBatch:
 
     def execute_parts(self, input: Buffer, output: Buffer, parts: int, sequential: bool = False,
                       stream=None) -> None:
-        """Runs only the CTA-queue lines (parts=1), the cluster lines
-        (parts=2) or both (3)."""
+        """Runs a subset of the lines: bit 0 the CTA-queue lines, bit 1 the
+        cluster lines, bit 2 the column/row passes of the long lines."""
         ip, ib = _buf(input)
         op, ob = _buf(output)
         _check(lib().b2f_batch_execute_parts(self._ptr, _stream(stream), ip, ib, op, ob, parts,

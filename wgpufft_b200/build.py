@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import concurrent.futures
 import os
+import re
 import subprocess
 import sys
 
@@ -21,19 +22,33 @@ def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu") or f.endswith(".cpp"))
 
 
-def _headers_mtime() -> float:
-    m = 0.0
-    for d in (CSRC, os.path.join(HERE, "..", "include")):
-        for f in os.listdir(d):
-            if f.endswith((".h", ".cuh")):
-                m = max(m, os.path.getmtime(os.path.join(d, f)))
+_INCLUDE = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
+_DIRS = (CSRC, os.path.join(HERE, "..", "include"))
+
+
+def _deps_mtime(path: str, seen=None) -> float:
+    """Newest modification time of a source and the local headers it
+    includes, recursively."""
+    seen = set() if seen is None else seen
+    if path in seen:
+        return 0.0
+    seen.add(path)
+    m = os.path.getmtime(path)
+    with open(path, encoding="utf-8") as f:
+        text = f.read()
+    for name in _INCLUDE.findall(text):
+        for d in (os.path.dirname(path),) + _DIRS:
+            cand = os.path.join(d, name)
+            if os.path.exists(cand):
+                m = max(m, _deps_mtime(cand, seen))
+                break
     return m
 
 
-def _compile(src: str, hdr_mtime: float, verbose: bool) -> str:
+def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, src + ".o")
     path = os.path.join(CSRC, src)
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), hdr_mtime):
+    if os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(path):
         return obj
     cmd = [NVCC] + CFLAGS + ["-c", path, "-o", obj]
     if verbose:
@@ -46,10 +61,9 @@ def _compile(src: str, hdr_mtime: float, verbose: bool) -> str:
 
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    hdr = _headers_mtime()
     srcs = _sources()
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        objs = list(ex.map(lambda s: _compile(s, hdr, verbose), srcs))
+        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [NVCC] + ARCH + ["-shared", "-cudart=static", "-o", LIB] + objs

@@ -3,6 +3,7 @@
 // transforms share persistent launches driven by a device work queue; the
 // reference has no counterpart (it records one dispatch chain per plan).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -10,6 +11,7 @@
 #include <thread>
 
 #include "batch.cuh"
+#include "longpass.cuh"
 #include "hostfft.h"
 #include "plan.h"
 
@@ -90,8 +92,16 @@ struct BatchPlan {
   unsigned int* d_counters = nullptr;  // [0] CTA queue, [1] cluster queue
   std::vector<void*> tables;
   uint32_t n_cta = 0, n_cl = 0, n_big = 0;
-  uint32_t phase_first[4] = {0, 0, 0, 0}, phase_count[4] = {0, 0, 0, 0};  // CTA-queue launches
-  uint64_t* d_line_scratch = nullptr;
+  // long lines (k_long_pass): length descriptors, lines, and the tasks of
+  // the column, row and Bluestein inverse-column phases, one launch each
+  LongLenDesc* d_long_lens = nullptr;
+  LongLine* d_long_lines = nullptr;
+  LongTask* d_long_tasks = nullptr;
+  uint32_t long_first[3] = {0, 0, 0}, long_count[3] = {0, 0, 0};
+  uint32_t long_cap = 0;
+  size_t smem_long = 0;
+  unsigned grid_long = 0;
+  uint64_t lines_long = 0, elems_long = 0;
   unsigned grid_big = 0;
   uint32_t buf_cta = 0, buf_cl = 0;
   size_t smem_cta = 0, smem_cl = 0;
@@ -101,8 +111,7 @@ struct BatchPlan {
   // description
   uint64_t lines_cta = 0, lines_cl = 0, distinct = 0, table_bytes = 0;
   uint64_t elems_cta = 0, elems_cl = 0;
-  uint64_t slot_elems = 0;  // BK_LONG scratch slot per CTA
-  c32* d_scratch = nullptr;
+  c32* d_scratch = nullptr;  // long lines: M values per line
   c32* d_tw = nullptr;
   uint64_t tw_bytes = 0;
   uint64_t scratch_bytes = 0;
@@ -119,7 +128,9 @@ struct BatchPlan {
     cudaFree(d_counters);
     cudaFree(d_scratch);
     cudaFree(d_tw);
-    cudaFree(d_line_scratch);
+    cudaFree(d_long_lens);
+    cudaFree(d_long_lines);
+    cudaFree(d_long_tasks);
     if (side) cudaStreamDestroy(side);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
@@ -130,6 +141,9 @@ struct BatchPlan {
 constexpr int kClusterP = 8;
 constexpr int kClusterBig = 16;  // non-portable cluster size for the longest Bluestein lines
 constexpr unsigned kCtaThreads = 256;
+// work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
+// cluster queues, [4 + ph] long-line phase ph
+constexpr unsigned kBatchCounters = 8;
 constexpr unsigned kClusterThreads = 512;
 
 struct LenInfo {
@@ -137,26 +151,55 @@ struct LenInfo {
   std::vector<cd> bhat;
   std::vector<uint32_t> pin, pout;
   double cost = 0;
+  LongLenDesc lng;      // long kinds
+  Schedule s1, s2;      // long kinds: schedules of N1 and N2
 };
 
-static bool pow2u(uint64_t v) { return v && !(v & (v - 1)); }
 
-// Line groups of the two passes of a long line: power-of-two passes run the
-// register path with 2048 points per group (128 threads with 16 values
-// each); other passes the shared-memory engine with 8 (or fewer) lines.
-static void set_long_groups(BatchLen& d) {
-  auto lg_of = [](uint32_t n, bool reg) -> uint32_t {
-    if (reg) {
-      uint32_t g = 2048 / n, l = 0;
-      while ((1u << (l + 1)) <= g) ++l;
-      return l;
+// Lines per task of a long-line pass of length nx (log2): 16 up to 208
+// points, 8 up to 393, 4 up to 512, so that a task's buffer of nx*(G+1)
+// values stays within 3540 (three buffers and the two table areas of two
+// CTAs fit one SM).
+static uint32_t long_lines_log2(uint64_t nx) { return nx <= 208 ? 4 : (nx <= 393 ? 3 : 2); }
+
+// T = N1 * N2 with both factors in [2, 512]: the split whose passes take
+// the most lines per task, then the most balanced; 0 when none exists.
+static uint64_t long_split(uint64_t T) {
+  uint64_t best_a = 0;
+  double best = 1e300;
+  for (uint64_t a = 2; a <= 512; ++a) {
+    if (T % a || T / a > 512 || T / a < 2) continue;
+    const uint64_t b = T / a;
+    const double score = 8.0 * ((4 - long_lines_log2(a)) + (4 - long_lines_log2(b))) +
+                         std::fabs(std::log((double)a) - std::log((double)b));
+    if (score < best) {
+      best = score;
+      best_a = a;
     }
-    return n <= 128 ? 4 : (n <= 256 ? 3 : 2);
-  };
-  d.reg1 = pow2u(d.N1) && d.N1 >= 16 && d.N1 <= 512;
-  d.reg2 = pow2u(d.N2) && d.N2 >= 16 && d.N2 <= 512;
-  d.lg = lg_of(d.N1, d.reg1);
-  d.lg2 = lg_of(d.N2, d.reg2);
+  }
+  return best_a;
+}
+
+// Long-line descriptor of length N over the transform length T = n1 * (T / n1)
+// (pass lengths <= 512, so at most 9 stages each).
+static void set_long(LenInfo& li, uint64_t N, uint64_t T, uint64_t n1, bool blue) {
+  BatchLen& d = li.d;
+  LongLenDesc& g = li.lng;
+  std::memset(&g, 0, sizeof(g));
+  d.kind = blue ? BK_LONG_BLUE : BK_LONG;
+  d.M = (uint32_t)T;
+  d.G = 1;
+  g.N = (uint32_t)N;
+  g.M = (uint32_t)T;
+  g.N1 = (uint32_t)n1;
+  g.N2 = (uint32_t)(T / n1);
+  g.lgc = long_lines_log2(g.N1);
+  g.lgr = long_lines_log2(g.N2);
+  g.blue = blue ? 1u : 0u;
+  g.scale = d.scale;
+  g.dN2 = make_fastdiv(g.N2);
+  li.s1 = schedule_for(g.N1);
+  li.s2 = schedule_for(g.N2);
 }
 
 // Chooses the execution of one distinct length.
@@ -174,26 +217,8 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
   d.scale = sc;
   d.dN = make_fastdiv((uint32_t)N);
   const auto cta_bytes = [](uint64_t lbuf) { return 2 * (size_t)ld_f32(lbuf) * 8; };
-  // long lines run as two passes of T = N1 * N2 (both <= 512) inside one
-  // CTA; the most balanced split of T, 0 when none exists
-  // (power-of-two factors, which take the register path, count double)
-  const auto split = [](uint64_t Tl) -> uint64_t {
-    uint64_t best_a = 0;
-    double best = 1e300;
-    for (uint64_t a = 2; a <= 512; ++a) {
-      if (Tl % a || Tl / a > 512 || Tl / a < 2) continue;
-      const uint64_t b2 = Tl / a;
-      double score = std::fabs(std::log((double)a) - std::log((double)b2));
-      score -= 4.0 * ((pow2u(a) && a >= 16) + (pow2u(b2) && b2 >= 16));
-      if (score < best) {
-        best = score;
-        best_a = a;
-      }
-    }
-    return best_a;
-  };
   uint64_t n1 = 0;
-  if (is_smooth13(N) && cta_bytes(N) > cta_cap && !clusters) n1 = split(N);
+  if (is_smooth13(N) && cta_bytes(N) > cta_cap && !clusters) n1 = long_split(N);
   uint32_t cl_split = 0;
   if (clusters && is_smooth13(N) && cta_bytes(N) > cta_cap)
     for (uint32_t P : {8u, 7u, 5u, 4u, 3u, 2u})
@@ -219,16 +244,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     d.LD = ld_f32(N);
     d.sch = schedule_for(N);
   } else if (smooth) {
-    d.kind = BK_LONG;
-    d.M = (uint32_t)N;
-    d.N1 = (uint32_t)n1;
-    d.N2 = (uint32_t)(N / n1);
-    d.LD1 = ld_f32(d.N1);
-    d.LD2 = ld_f32(d.N2);
-    d.LD = std::max(d.LD1, d.LD2);
-    set_long_groups(d);
-    d.sch = schedule_for(d.N1);
-    d.sch2 = schedule_for(d.N2);
+    set_long(li, N, N, n1, false);
   } else if (is_prime_u64(N) && N >= 3 && is_smooth13(N - 1) && cta_bytes(N) <= cta_cap) {
     d.kind = BK_RADER;
     d.M = (uint32_t)(N - 1);
@@ -258,11 +274,9 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     uint64_t mlong = 0, a = 0;
     if (cta_bytes(M) > cta_cap && !clusters) {
       // the smallest 7-smooth convolution length that splits into factors <= 512
-      // (a power-of-two length would put both passes on the register path,
-      // but its extra points cost more than the register path saves)
       for (uint64_t m = 2 * N - 1; !mlong && m <= 262144; ++m) {
         if (!smooth7(m)) continue;
-        a = split(m);
+        a = long_split(m);
         if (a) {
           mlong = m;
           break;
@@ -276,16 +290,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
       d.sch = schedule_for(M);
     } else if (mlong) {
       M = mlong;
-      d.kind = BK_LONG_BLUE;
-      d.M = (uint32_t)M;
-      d.N1 = (uint32_t)a;
-      d.N2 = (uint32_t)(M / a);
-      d.LD1 = ld_f32(d.N1);
-      d.LD2 = ld_f32(d.N2);
-      d.LD = std::max(d.LD1, d.LD2);
-      set_long_groups(d);
-      d.sch = schedule_for(d.N1);
-      d.sch2 = schedule_for(d.N2);
+      set_long(li, N, M, a, true);
     } else {
       // cluster Bluestein: convolution P*L >= 2N-1, L 7-smooth and fitting
       uint32_t P = kClusterP;
@@ -408,15 +413,25 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     std::map<uint32_t, uint32_t> cache;
     for (auto& li : infos) {
       BatchLen& d = li.d;
-      attach_stage_table(d.sch, tw, cache);
       if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
-        attach_stage_table(d.sch2, tw, cache);
-        d.ta = (uint32_t)tw.size();
-        for (uint32_t a = 0; a < d.N1; ++a) tw.push_back(root_fwd((uint64_t)a * d.N2, d.M));
-        d.tb = (uint32_t)tw.size();
-        for (uint32_t c = 0; c < d.N2; ++c) tw.push_back(root_fwd(c, d.M));
-        d.dB = make_fastdiv(d.N2);
-      } else if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) {
+        // stage tables of both passes and W_M^{a N2} / W_M^b
+        LongLenDesc& g = li.lng;
+        attach_stage_table(li.s1, tw, cache);
+        attach_stage_table(li.s2, tw, cache);
+        for (int w = 0; w < 2; ++w) {
+          const Schedule& sc = w ? li.s2 : li.s1;
+          LongSched& ls = w ? g.s2 : g.s1;
+          ls.nst = sc.nst;
+          for (uint32_t k = 0; k < sc.nst; ++k) ls.st[k] = sc.st[k];
+        }
+        g.ta = (uint32_t)tw.size();
+        for (uint32_t a = 0; a < g.N1; ++a) tw.push_back(root_fwd((uint64_t)a * g.N2, g.M));
+        g.tb = (uint32_t)tw.size();
+        for (uint32_t c = 0; c < g.N2; ++c) tw.push_back(root_fwd(c, g.M));
+        continue;
+      }
+      attach_stage_table(d.sch, tw, cache);
+      if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) {
         d.ta = (uint32_t)tw.size();
         for (uint32_t a = 0; a < d.P; ++a) tw.push_back(root_fwd((uint64_t)a * d.L, d.M));
         d.tb = (uint32_t)tw.size();
@@ -457,6 +472,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       void* p;
       if (!upload(f.data(), f.size() * 4, &p)) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch table allocation failed");
       li.d.bhat = (const c32*)p;
+      li.lng.bhat = (const c32*)p;
     }
     if (!li.pin.empty()) {
       void *a, *b;
@@ -470,48 +486,30 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   std::vector<uint64_t> sorted_off;
   std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks;
   std::vector<double> cta_cost, cl_cost, big_cost;
-  (void)0;
-  std::vector<uint32_t> order_len(lens_list.size());
-  for (size_t i = 0; i < lens_list.size(); ++i) order_len[i] = (uint32_t)i;
-  // lines sorted by length index; tasks reference contiguous runs.  Long
-  // lines become phase tasks: one task per column or row group, phase 1
-  // (with the short tasks) then 2, 3, 4 in later launches.
-  std::vector<BatchTask> phase_tasks[4];
-  std::vector<uint64_t> line_scratch;
+  // lines sorted by length index; CTA tasks reference contiguous runs.
+  // Long lines get one task per column or row group in each of their
+  // phases (1: columns, 2: rows, 3: Bluestein inverse columns).
+  std::vector<LongLine> long_lines;
+  std::vector<LongTask> long_tasks[3];
   uint64_t scratch_total = 0;
   for (size_t li = 0; li < lens_list.size(); ++li) {
     const auto& lines = by_len[lens_list[li]];
     const BatchLen& d = infos[li].d;
     bp->kind_lines[d.kind] += lines.size();
     const bool cl = d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE;
-    const bool lng = d.kind == BK_LONG || d.kind == BK_LONG_BLUE;
-    if (lng) {
-      const int nph = d.kind == BK_LONG_BLUE ? 4 : 2;
+    if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
+      const LongLenDesc& g = infos[li].lng;
+      const uint32_t Gc = 1u << g.lgc, Gr = 1u << g.lgr;
       for (uint64_t line : lines) {
-        const uint32_t idx = (uint32_t)sorted_off.size();
-        sorted_off.push_back(offsets[line]);
-        line_scratch.resize(idx + 1, 0);
-        line_scratch[idx] = scratch_total;
-        scratch_total += (d.kind == BK_LONG_BLUE ? 2ull : 1ull) * d.M;
-        bp->elems_cta += lens_list[li];
-        bp->lines_cta += 1;
-        for (int ph = 1; ph <= nph; ++ph) {
-          const uint32_t extent = (ph % 2 == 1) ? d.N2 : d.N1;  // column passes walk N2
-          const uint32_t Gp = (ph % 2 == 1) ? (1u << d.lg) : (1u << d.lg2);
-          for (uint32_t g0 = 0; g0 < extent; g0 += Gp) {
-            BatchTask t;
-            t.len = (uint32_t)li;
-            t.first = idx;
-            t.count = g0;
-            t.pad = (uint32_t)ph;
-            if (ph == 1) {
-              cta_tasks.push_back(t);
-              cta_cost.push_back((double)Gp * (ph % 2 == 1 ? d.N1 : d.N2) * 8.0);
-            } else {
-              phase_tasks[ph - 1].push_back(t);
-            }
-          }
-        }
+        const uint32_t idx = (uint32_t)long_lines.size();
+        long_lines.push_back(LongLine{offsets[line], scratch_total, (uint32_t)li, 0});
+        scratch_total += g.M;
+        bp->elems_long += lens_list[li];
+        bp->lines_long += 1;
+        for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) long_tasks[0].push_back(LongTask{idx, g0});
+        for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr) long_tasks[1].push_back(LongTask{idx, g0});
+        if (g.blue)
+          for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) long_tasks[2].push_back(LongTask{idx, g0});
       }
       continue;
     }
@@ -522,7 +520,6 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       t.count = (uint32_t)std::min<size_t>(cl ? 1 : d.G, lines.size() - s);
       t.pad = 0;
       for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[lines[s + c]]);
-      line_scratch.resize(sorted_off.size(), 0);
       if (cl && d.P == kClusterBig) {
         big_tasks.push_back(t);
         big_cost.push_back(infos[li].cost);
@@ -561,11 +558,13 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   for (auto& li : infos) {
     const BatchLen& d = li.d;
     if (d.kind == BK_CL_MIXED || d.kind == BK_CL_BLUE) buf_cl = std::max(buf_cl, d.LD);
-    else if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE)
-      buf_cta = std::max<uint32_t>(buf_cta, std::max((1u << d.lg) * d.LD1, (1u << d.lg2) * d.LD2));
-    else buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
-    if (d.kind == BK_LONG) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, d.N);
-    if (d.kind == BK_LONG_BLUE) bp->slot_elems = std::max<uint64_t>(bp->slot_elems, 2ull * d.M);
+    else if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
+      const LongLenDesc& g = li.lng;
+      bp->long_cap = std::max(bp->long_cap, g.N1 * ((1u << g.lgc) + 1));
+      bp->long_cap = std::max(bp->long_cap, g.N2 * ((1u << g.lgr) + 1));
+    } else {
+      buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
+    }
   }
   bp->buf_cta = buf_cta;
   bp->buf_cl = buf_cl;
@@ -575,28 +574,40 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   std::vector<BatchLen> dl(infos.size());
   for (size_t i = 0; i < infos.size(); ++i) dl[i] = infos[i].d;
   std::vector<BatchTask> all = cta_tasks;
-  bp->phase_first[0] = 0;
-  bp->phase_count[0] = (uint32_t)cta_tasks.size();
-  for (int ph = 1; ph < 4; ++ph) {
-    bp->phase_first[ph] = (uint32_t)all.size();
-    bp->phase_count[ph] = (uint32_t)phase_tasks[ph].size();
-    all.insert(all.end(), phase_tasks[ph].begin(), phase_tasks[ph].end());
-  }
-  bp->n_cta = (uint32_t)all.size();
   all.insert(all.end(), cl_tasks.begin(), cl_tasks.end());
   all.insert(all.end(), big_tasks.begin(), big_tasks.end());
   bool okc = cudaMalloc(&bp->d_lens, dl.size() * sizeof(BatchLen)) == cudaSuccess &&
              cudaMalloc(&bp->d_tasks, std::max<size_t>(1, all.size()) * sizeof(BatchTask)) == cudaSuccess &&
              cudaMalloc(&bp->d_off, sorted_off.size() * 8) == cudaSuccess &&
-             cudaMalloc(&bp->d_counters, 8 * sizeof(unsigned int)) == cudaSuccess;
+             cudaMalloc(&bp->d_counters, kBatchCounters * sizeof(unsigned int)) == cudaSuccess;
   if (!okc) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
   cudaMemcpy(bp->d_lens, dl.data(), dl.size() * sizeof(BatchLen), cudaMemcpyHostToDevice);
   if (!all.empty()) cudaMemcpy(bp->d_tasks, all.data(), all.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
   cudaMemcpy(bp->d_off, sorted_off.data(), sorted_off.size() * 8, cudaMemcpyHostToDevice);
-  line_scratch.resize(sorted_off.size(), 0);
-  if (cudaMalloc(&bp->d_line_scratch, line_scratch.size() * 8) != cudaSuccess)
-    return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
-  cudaMemcpy(bp->d_line_scratch, line_scratch.data(), line_scratch.size() * 8, cudaMemcpyHostToDevice);
+  // long lines: descriptors (indexed like the length table), lines, tasks
+  if (!long_lines.empty()) {
+    std::vector<LongLenDesc> gl(infos.size());
+    std::memset(gl.data(), 0, gl.size() * sizeof(LongLenDesc));
+    for (size_t i = 0; i < infos.size(); ++i)
+      if (infos[i].d.kind == BK_LONG || infos[i].d.kind == BK_LONG_BLUE) gl[i] = infos[i].lng;
+    std::vector<LongTask> lt;
+    for (int ph = 0; ph < 3; ++ph) {
+      bp->long_first[ph] = (uint32_t)lt.size();
+      bp->long_count[ph] = (uint32_t)long_tasks[ph].size();
+      lt.insert(lt.end(), long_tasks[ph].begin(), long_tasks[ph].end());
+    }
+    const bool okl =
+        cudaMalloc(&bp->d_long_lens, gl.size() * sizeof(LongLenDesc)) == cudaSuccess &&
+        cudaMalloc(&bp->d_long_lines, long_lines.size() * sizeof(LongLine)) == cudaSuccess &&
+        cudaMalloc(&bp->d_long_tasks, lt.size() * sizeof(LongTask)) == cudaSuccess &&
+        cudaMalloc(&bp->d_scratch, scratch_total * 8) == cudaSuccess;
+    if (!okl) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch long-line allocation failed");
+    bp->scratch_bytes = scratch_total * 8;
+    cudaMemcpy(bp->d_long_lens, gl.data(), gl.size() * sizeof(LongLenDesc), cudaMemcpyHostToDevice);
+    cudaMemcpy(bp->d_long_lines, long_lines.data(), long_lines.size() * sizeof(LongLine),
+               cudaMemcpyHostToDevice);
+    cudaMemcpy(bp->d_long_tasks, lt.data(), lt.size() * sizeof(LongTask), cudaMemcpyHostToDevice);
+  }
   // launch shapes
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
@@ -606,14 +617,18 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_cta, kCtaThreads, bp->smem_cta);
     per_sm = std::max(per_sm, 1);
-    uint32_t most = 0;
-    for (int ph = 0; ph < 4; ++ph) most = std::max(most, bp->phase_count[ph]);
-    bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, std::max<uint32_t>(most, 1));
-    if (scratch_total) {
-      bp->scratch_bytes = scratch_total * 8;
-      if (cudaMalloc(&bp->d_scratch, bp->scratch_bytes) != cudaSuccess)
-        return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch scratch allocation failed");
-    }
+    bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, bp->n_cta);
+  }
+  if (!long_lines.empty()) {
+    bp->smem_long = (3 * (size_t)bp->long_cap + 2 * kLongTab) * 8;
+    if (set_smem(k_long_pass, bp->smem_long) != cudaSuccess)
+      return fail(B2F_ERR_DEVICE, "long-line kernel shared memory");
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_long_pass, kLongThreads, bp->smem_long);
+    per_sm = std::max(per_sm, 1);
+    uint32_t most = std::max(bp->long_count[0], std::max(bp->long_count[1], bp->long_count[2]));
+    bp->grid_long = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm,
+                                                 (most + kLongChunk - 1) / kLongChunk);
   }
   if (bp->n_cl) {
     if (set_smem(k_batch_cluster<kClusterP>, bp->smem_cl) != cudaSuccess)
@@ -670,8 +685,13 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   os << "{\"lines\":" << nlines << ",\"distinct_lengths\":" << bp->distinct
      << ",\"cta_lines\":" << bp->lines_cta << ",\"cluster_lines\":" << bp->lines_cl
      << ",\"cta_elements\":" << bp->elems_cta << ",\"cluster_elements\":" << bp->elems_cl
-     << ",\"cta_tasks\":" << bp->n_cta << ",\"cta_launches\":"
-     << ((bp->phase_count[0] > 0) + (bp->phase_count[1] > 0) + (bp->phase_count[2] > 0) + (bp->phase_count[3] > 0)) << ",\"cluster_tasks\":" << bp->n_cl
+     << ",\"long_lines\":" << bp->lines_long << ",\"long_elements\":" << bp->elems_long
+     << ",\"cta_tasks\":" << bp->n_cta << ",\"cta_launches\":" << (bp->n_cta > 0)
+     << ",\"long_tasks\":[" << bp->long_count[0] << "," << bp->long_count[1] << ","
+     << bp->long_count[2] << "],\"long_launches\":"
+     << ((bp->long_count[0] > 0) + (bp->long_count[1] > 0) + (bp->long_count[2] > 0))
+     << ",\"long_grid\":" << bp->grid_long << ",\"long_threads\":" << kLongThreads
+     << ",\"long_smem\":" << bp->smem_long << ",\"cluster_tasks\":" << bp->n_cl
      << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
      << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
      << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5]
@@ -690,21 +710,18 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
 }
 
 static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in, void* out,
-                            uint32_t parts = 3, bool sequential = false) {
+                            uint32_t parts = 7, bool sequential = false) {
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != bp.device) cudaSetDevice(bp.device);
-  cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, 8 * sizeof(unsigned int), st);
+  cudaError_t e = cudaMemsetAsync(bp.d_counters, 0, kBatchCounters * sizeof(unsigned int), st);
   BatchParams p{};
   p.in = (const c32*)in;
   p.out = (c32*)out;
   p.lens = bp.d_lens;
   p.line_off = bp.d_off;
   p.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
-  p.scratch = bp.d_scratch;
-  p.line_scratch = bp.d_line_scratch;
   p.tw = bp.d_tw;
-  p.slot_elems = bp.slot_elems;
   const bool run_cl = (bp.n_cl || bp.n_big) && (parts & 2);
   const bool run_cta = bp.n_cta && (parts & 1);
   cudaStream_t cl_stream = sequential ? st : bp.side;
@@ -742,13 +759,30 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
     }
   }
   if (e == cudaSuccess && run_cta) {
-    for (int ph = 0; ph < 4 && e == cudaSuccess; ++ph) {
-      if (bp.phase_count[ph] == 0) continue;
-      BatchParams pt = p;
-      pt.tasks = bp.d_tasks + bp.phase_first[ph];
-      pt.ntasks = bp.phase_count[ph];
-      pt.counter = bp.d_counters + 4 + ph;
-      k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+    BatchParams pt = p;
+    pt.tasks = bp.d_tasks;
+    pt.ntasks = bp.n_cta;
+    pt.counter = bp.d_counters;
+    k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && (parts & 4) && bp.lines_long) {
+    LongParams lp{};
+    lp.in = (const c32*)in;
+    lp.out = (c32*)out;
+    lp.scratch = bp.d_scratch;
+    lp.tw = bp.d_tw;
+    lp.lens = bp.d_long_lens;
+    lp.lines = bp.d_long_lines;
+    lp.inverse = p.inverse;
+    lp.cap = bp.long_cap;
+    for (uint32_t ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
+      if (bp.long_count[ph] == 0) continue;
+      lp.tasks = bp.d_long_tasks + bp.long_first[ph];
+      lp.ntasks = bp.long_count[ph];
+      lp.phase = ph + 1;
+      lp.counter = bp.d_counters + 4 + ph;
+      k_long_pass<<<bp.grid_long, kLongThreads, bp.smem_long, st>>>(lp);
       e = cudaGetLastError();
     }
   }

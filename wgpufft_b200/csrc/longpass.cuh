@@ -1,0 +1,463 @@
+// Long lines of a batch (a line, or a Bluestein convolution, too long for
+// one CTA's shared memory): two or three HBM passes of a persistent kernel.
+//
+// A length T = N1 * N2 FFT (T = N, or the convolution length M) runs as
+//   column pass: for each n2, FFT_N1 over n1 of x[N2 n1 + n2], times
+//                W_T^{n2 k1}, into the scratch row k1 (natural [k1][n2]);
+//   row pass:    for each k1, FFT_N2 over n2 of scratch row k1, giving
+//                X[k1 + N1 k2].
+// A task is G (16, 8 or 4) adjacent columns or rows of one line, so every
+// global access is a segment of G consecutive complex values (128 bytes at
+// G = 16): rows of columns n2..n2+G-1, or the outputs k1..k1+G-1 of one k2.
+// The G lines of a task sit interleaved in shared memory, element (i, l) at
+// i*(G+1) + l: the 16 threads of a half-warp take the same position i of 16
+// lines, so the Stockham stages and the column segments are conflict-free,
+// and the pitch G+1 keeps the transposed row loads (consecutive i, fixed l)
+// conflict-free too.  Each thread keeps one line l and walks the butterflies
+// j = s, s+S, ... of every stage with incrementally updated offsets.
+//
+// Bluestein lines (convolution M = N1 N2) take three passes: the chirped
+// column pass; a middle row pass that runs the forward row FFT, multiplies
+// by the chirp spectrum, and runs the row half of the inverse FFT
+// (y[N2 n1 + n2] = sum_k1 W_N1^{-n1 k1} W_M^{-n2 k1} sum_k2 W_N2^{-n2 k2} Y[k1 + N1 k2],
+// computed on conjugates with the forward codelets) in place on the rows;
+// and the inverse column pass, chirped into the output.  One scratch region
+// of M values per line.
+//
+// Loads are asynchronous (cp.async): while a CTA transforms one task, the
+// copies of its next task are already in flight into the other landing
+// buffer, together with the twiddle tables of its length (stage twiddles,
+// W_M^{a N2} and W_M^b) when they differ from the ones that buffer last
+// held.  The work queue hands out chunks of consecutive tasks (mostly one
+// line), so the tables change rarely; nothing waits on another CTA.
+#pragma once
+#include "batch.cuh"
+
+namespace b2f {
+
+constexpr uint32_t kLongThreads = 256;
+constexpr int kLongMaxStages = 10;  // pass lengths <= 512
+constexpr uint32_t kLongChunk = 4;  // consecutive tasks per work-queue claim
+// table area of one landing buffer (complex values): stage twiddles of the
+// pass (length - 1 <= 511), W_M^{a N2} (a < N1 <= 512), W_M^b (b < N2 <= 512)
+constexpr uint32_t kTabSt = 0, kTabTa = 512, kTabTb = 1024;
+constexpr uint32_t kLongTab = 1536;
+
+enum LongPassKind : uint32_t {
+  LP_COL = 0,    // smooth line, column pass: x -> scratch
+  LP_ROW = 1,    // smooth line, row pass: scratch -> out
+  LP_BCOL1 = 2,  // Bluestein, chirped column pass: x -> scratch
+  LP_BMID = 3,   // Bluestein, rows: FFT, spectrum product, inverse-row FFT, in place
+  LP_BCOL3 = 4,  // Bluestein, inverse column pass, chirped: scratch -> out
+};
+
+struct LongSched {
+  uint32_t nst;
+  StageDesc st[kLongMaxStages];
+};
+
+struct LongLenDesc {
+  uint32_t N, M, N1, N2;
+  uint32_t lgc, lgr;  // log2 of the lines per column / row task
+  uint32_t blue;
+  float scale;
+  const c32* bhat;    // Bluestein: spectrum of the conjugate chirp / M, natural order
+  uint32_t ta, tb;    // W_M^{a N2} (a < N1), W_M^b (b < N2): offsets into the twiddle table
+  FastDiv dN2;
+  LongSched s1, s2;   // schedules of N1 (columns) and N2 (rows)
+};
+
+struct LongLine {
+  uint64_t base;     // complex offset of the line in the input and output buffers
+  uint64_t scratch;  // complex offset of its scratch region (M values)
+  uint32_t len;      // index into the length table
+  uint32_t pad;
+};
+
+struct LongTask {
+  uint32_t line;
+  uint32_t g0;  // first column (column passes) or row (row passes) of the task
+};
+
+struct LongParams {
+  const c32* in;
+  c32* out;
+  c32* scratch;
+  const c32* tw;
+  const LongLenDesc* lens;
+  const LongLine* lines;
+  const LongTask* tasks;
+  uint32_t ntasks;
+  uint32_t phase;    // 1: column pass, 2: row pass, 3: Bluestein inverse columns
+  uint32_t inverse;
+  uint32_t cap;      // complex elements per shared-memory buffer
+  unsigned int* counter;
+};
+
+// cp.async of 8 bytes, zero-filled (nothing read) when !valid.
+FFT_D void cp_async8_zfill(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const unsigned n = valid ? 8u : 0u;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
+               : "memory");
+}
+FFT_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+FFT_D void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+FFT_D uint32_t long_kind(uint32_t phase, bool blue) {
+  if (phase == 1) return blue ? LP_BCOL1 : LP_COL;
+  if (phase == 2) return blue ? LP_BMID : LP_ROW;
+  return LP_BCOL3;
+}
+
+// W^j from a two-level table: j = a*B + b, value ta[a] * tb[b].
+FFT_D c32 tw_two(const c32* __restrict__ tw, uint32_t ta, uint32_t tb, uint32_t j,
+                 const FastDiv& dB) {
+  const uint32_t a = fdiv(j, dB), b = j - a * dB.d;
+  return cmul(tw[ta + a], tw[tb + b]);
+}
+
+// One radix-R stage over G interleaved lines, src -> dst: thread (l, s)
+// runs the butterflies j = s, s+S, ... of line l; k = j mod Ns advances by
+// S mod Ns.  tws: this stage's twiddles, row k at k*(R-1).
+template <int R>
+FFT_D void ilv_stage(const c32* __restrict__ src, c32* __restrict__ dst, const StageDesc& sd,
+                     uint32_t lg, uint32_t tid, const c32* __restrict__ tws) {
+  const uint32_t G = 1u << lg, P = G + 1;
+  const uint32_t l = tid & (G - 1), s = tid >> lg, S = kLongThreads >> lg;
+  const uint32_t NR = sd.NR, Ns = sd.Ns;
+  if (s >= NR) return;
+  const uint32_t qs = NR * P, rs = Ns * P;
+  uint32_t k = 0, kinc = 0;
+  if (Ns > 1) {
+    k = s - fdiv(s, sd.dNs) * Ns;
+    kinc = S - fdiv(S, sd.dNs) * Ns;
+  }
+#pragma unroll 1
+  for (uint32_t j = s; j < NR; j += S) {
+    const c32* sb = src + j * P + l;
+    c32 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = sb[q * qs];
+    if (Ns > 1) {
+      const c32* t = tws + k * (R - 1);
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], t[q - 1]);
+    }
+    dft<float, R>(v);
+    c32* db = dst + ((j - k) * R + k) * P + l;
+#pragma unroll
+    for (int r = 0; r < R; ++r) db[r * rs] = v[r];
+    k += kinc;
+    if (k >= Ns) k -= Ns;
+  }
+}
+
+// The whole schedule, a <-> b; returns the buffer holding the result.  T:
+// the table area (stage twiddles from offset kTabSt, global table offsets
+// relative to the first stage's).  The caller synchronises before; every
+// stage ends with a barrier.
+FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t tid,
+                   const c32* T) {
+  const uint32_t tw0 = sch.st[0].tw_off;
+#pragma unroll 1
+  for (uint32_t s = 0; s < sch.nst; ++s) {
+    const StageDesc& sd = sch.st[s];
+    const c32* tws = T + kTabSt + (sd.tw_off - tw0);
+    switch (sd.R) {
+      case 2: ilv_stage<2>(a, b, sd, lg, tid, tws); break;
+      case 3: ilv_stage<3>(a, b, sd, lg, tid, tws); break;
+      case 4: ilv_stage<4>(a, b, sd, lg, tid, tws); break;
+      case 5: ilv_stage<5>(a, b, sd, lg, tid, tws); break;
+      case 7: ilv_stage<7>(a, b, sd, lg, tid, tws); break;
+      case 8: ilv_stage<8>(a, b, sd, lg, tid, tws); break;
+      case 9: ilv_stage<9>(a, b, sd, lg, tid, tws); break;
+      case 11: ilv_stage<11>(a, b, sd, lg, tid, tws); break;
+      case 13: ilv_stage<13>(a, b, sd, lg, tid, tws); break;
+      case 16: ilv_stage<16>(a, b, sd, lg, tid, tws); break;
+      default: break;
+    }
+    __syncthreads();
+    c32* t = a;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Chirp exp(-i pi n^2 / N) at n, n + D, n + 2D, ... : q = n^2 mod 2N kept
+// incrementally ((n + D)^2 = n^2 + 2nD + D^2); value() = W_2N^q.
+struct ChirpWalk {
+  uint32_t q, u, dsq, u2, twoN;
+  FFT_D void init(uint64_t n, uint32_t D, uint32_t N) {
+    twoN = 2 * N;
+    q = (uint32_t)((n * n) % twoN);
+    u = (uint32_t)((2 * n * (uint64_t)D) % twoN);
+    dsq = (uint32_t)(((uint64_t)D * D) % twoN);
+    u2 = (uint32_t)((2 * (uint64_t)D * D) % twoN);
+  }
+  FFT_D void step() {
+    q += u;
+    if (q >= twoN) q -= twoN;
+    q += dsq;
+    if (q >= twoN) q -= twoN;
+    u += u2;
+    if (u >= twoN) u -= twoN;
+  }
+  FFT_D c32 value() const { return twiddle_f32(q, twoN); }
+};
+
+FFT_D void copy_async(c32* dst, const c32* src, uint32_t n, uint32_t tid) {
+  for (uint32_t e = tid; e < n; e += kLongThreads) cp_async8_zfill(dst + e, src + e, true);
+}
+
+// Issues the copies of one task into the landing buffer X (zero-filled
+// where the task has no data) and, with tables, of its length's twiddle
+// tables into the table area T.
+FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongLine& ln, uint32_t g0,
+                      uint32_t kind, c32* X, c32* T, bool tables, uint32_t tid) {
+  const bool colk = kind == LP_COL || kind == LP_BCOL1 || kind == LP_BCOL3;
+  if (tables) {
+    const LongSched& sch = colk ? d.s1 : d.s2;
+    const uint32_t nx = colk ? d.N1 : d.N2;
+    copy_async(T + kTabSt, p.tw + sch.st[0].tw_off, nx - 1, tid);
+    if (kind == LP_COL || kind == LP_BCOL1 || kind == LP_BMID) {
+      copy_async(T + kTabTa, p.tw + d.ta, d.N1, tid);
+      copy_async(T + kTabTb, p.tw + d.tb, d.N2, tid);
+    }
+  }
+  if (colk) {
+    // columns g0..g0+G-1: row n1 is the segment src[N2 n1 + g0 + l]
+    const uint32_t lg = d.lgc, G = 1u << lg, P = G + 1;
+    const uint32_t l = tid & (G - 1), S = kLongThreads >> lg;
+    const uint32_t N2 = d.N2, Nx = d.N1;
+    const bool col_ok = g0 + l < N2;
+    const c32* src = (kind == LP_BCOL3) ? p.scratch + ln.scratch : p.in + ln.base;
+    const uint32_t lim = (kind == LP_BCOL1) ? d.N : d.M;  // chirped pass: zero beyond the line
+    uint32_t i = tid >> lg;
+    uint32_t n = N2 * i + g0 + l;
+    c32* dp = X + i * P + l;
+#pragma unroll 4
+    for (; i < Nx; i += S) {
+      const bool ok = col_ok && n < lim;
+      cp_async8_zfill(dp, ok ? src + n : src, ok);
+      n += S * N2;
+      dp += S * P;
+    }
+  } else {
+    // rows g0..g0+G-1 of the scratch: warp w copies rows w, w+8, ...
+    const uint32_t lg = d.lgr, G = 1u << lg, P = G + 1;
+    const uint32_t N2 = d.N2, N1 = d.N1;
+    const uint32_t w = tid >> 5, lane = tid & 31;
+    for (uint32_t r = w; r < G; r += kLongThreads / 32) {
+      const bool ok = g0 + r < N1;
+      const c32* row = p.scratch + ln.scratch + (uint64_t)(ok ? g0 + r : 0) * N2;
+      c32* dp = X + lane * P + r;
+#pragma unroll 4
+      for (uint32_t n2 = lane; n2 < N2; n2 += 32) {
+        cp_async8_zfill(dp, row + n2, ok);
+        dp += 32 * P;
+      }
+    }
+  }
+}
+
+// Transforms the task whose data sits in X (W: the ping-pong partner, T:
+// its table area) and stores its results.  Ends without a barrier.
+FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLine& ln, uint32_t g0,
+                        uint32_t kind, c32* X, c32* W, const c32* T, uint32_t tid) {
+  const bool inv = p.inverse != 0;
+  const bool colk = kind == LP_COL || kind == LP_BCOL1 || kind == LP_BCOL3;
+  const uint32_t lg = colk ? d.lgc : d.lgr, G = 1u << lg, P = G + 1;
+  const uint32_t l = tid & (G - 1), S = kLongThreads >> lg, i0 = tid >> lg;
+  const uint32_t N1 = d.N1, N2 = d.N2;
+  // input conjugation (inverse transforms) and the chirp of the first
+  // Bluestein pass, in place
+  if (kind == LP_BCOL1) {
+    const uint32_t c = g0 + l;
+    if (c < N2) {
+      uint32_t n = N2 * i0 + c;
+      ChirpWalk cw;
+      cw.init(n, S * N2, d.N);
+      c32* dp = X + i0 * P + l;
+      for (uint32_t i = i0; i < N1 && n < d.N; i += S) {
+        c32 v = *dp;
+        if (inv) v.im = -v.im;
+        *dp = cmul(v, cw.value());
+        cw.step();
+        n += S * N2;
+        dp += S * P;
+      }
+    }
+    __syncthreads();
+  } else if (kind == LP_COL && inv) {
+    for (uint32_t e = tid; e < N1 * P; e += kLongThreads) X[e].im = -X[e].im;
+    __syncthreads();
+  }
+  const LongSched& sch = colk ? d.s1 : d.s2;
+  c32* r = X;
+  c32* o = W;
+  // one FFT; the Bluestein middle pass runs two with the spectrum product
+  // (at k = k1 + N1 k2, k1 = g0 + l, k2 = i, conjugated) between them: the
+  // forward row FFT of the conjugate is the inverse row FFT
+  const int nfft = kind == LP_BMID ? 2 : 1;
+#pragma unroll 1
+  for (int f = 0; f < nfft; ++f) {
+    c32* res = ilv_fft(r, o, sch, lg, tid, T);
+    o = (res == r) ? o : r;
+    r = res;
+    if (f + 1 == nfft) break;
+    const uint32_t k1 = g0 + l;
+    if (k1 < N1) {
+      c32* dp = r + i0 * P + l;
+      const c32* bh = d.bhat + k1 + (uint64_t)N1 * i0;
+#pragma unroll 4
+      for (uint32_t i = i0; i < N2; i += S) {
+        c32 v = cmul(*dp, *bh);
+        v.im = -v.im;
+        *dp = v;
+        dp += S * P;
+        bh += (uint64_t)S * N1;
+      }
+    }
+    __syncthreads();
+  }
+  // stores
+  if (kind == LP_COL || kind == LP_BCOL1) {
+    // scratch[k1][g0 + l] = X[k1] * W_M^{(g0+l) k1}
+    const uint32_t c = g0 + l;
+    if (c < N2) {
+      c32* dst = p.scratch + ln.scratch + (uint64_t)N2 * i0 + c;
+      const c32* sp = r + i0 * P + l;
+#pragma unroll 4
+      for (uint32_t k1 = i0; k1 < N1; k1 += S) {
+        *dst = cmul(*sp, tw_two(T, kTabTa, kTabTb, c * k1, d.dN2));
+        dst += (uint64_t)S * N2;
+        sp += S * P;
+      }
+    }
+  } else if (kind == LP_ROW) {
+    // out[k1 + N1 k2], k1 = g0 + l
+    const uint32_t k1 = g0 + l;
+    if (k1 < N1) {
+      const float sc = d.scale;
+      c32* dst = p.out + ln.base + k1 + (uint64_t)N1 * i0;
+      const c32* sp = r + i0 * P + l;
+#pragma unroll 4
+      for (uint32_t k2 = i0; k2 < N2; k2 += S) {
+        c32 v = *sp;
+        v.re *= sc;
+        v.im = inv ? -v.im * sc : v.im * sc;
+        *dst = v;
+        dst += (uint64_t)S * N1;
+        sp += S * P;
+      }
+    }
+  } else if (kind == LP_BMID) {
+    // scratch row k1 = g0 + r, position n2: V * W_M^{n2 k1} (warp w writes rows w, w+8, ...)
+    const uint32_t w = tid >> 5, lane = tid & 31;
+    for (uint32_t rr = w; rr < G; rr += kLongThreads / 32) {
+      const uint32_t k1 = g0 + rr;
+      if (k1 >= N1) break;
+      c32* row = p.scratch + ln.scratch + (uint64_t)k1 * N2;
+      const c32* sp = r + lane * P + rr;
+#pragma unroll 4
+      for (uint32_t n2 = lane; n2 < N2; n2 += 32) {
+        row[n2] = cmul(*sp, tw_two(T, kTabTa, kTabTb, n2 * k1, d.dN2));
+        sp += 32 * P;
+      }
+    }
+  } else {  // LP_BCOL3: out[n] = conj(Y[n]) * chirp(n), n = N2 n1 + g0 + l < N
+    const uint32_t c = g0 + l;
+    if (c < N2) {
+      const float sc = d.scale;
+      uint32_t n = N2 * i0 + c;
+      ChirpWalk cw;
+      cw.init(n, S * N2, d.N);
+      c32* dst = p.out + ln.base + n;
+      const c32* sp = r + i0 * P + l;
+      for (uint32_t n1 = i0; n1 < N1 && n < d.N; n1 += S) {
+        c32 wv = *sp;
+        wv.im = -wv.im;
+        c32 v = cmul(wv, cw.value());
+        v.re *= sc;
+        v.im = inv ? -v.im * sc : v.im * sc;
+        *dst = v;
+        cw.step();
+        n += S * N2;
+        dst += (uint64_t)S * N2;
+        sp += S * P;
+      }
+    }
+  }
+}
+
+// Persistent kernel of one long-line phase.  Dynamic shared memory: two
+// landing buffers and one work buffer of p.cap complex values, then the two
+// table areas of kLongTab values (one per landing buffer).
+__global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_constant__ LongParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ LongLenDesc s_len[2];
+  __shared__ LongLine s_line[2];
+  __shared__ uint32_t s_g0[2];
+  __shared__ uint32_t s_claim;
+  c32* const base = reinterpret_cast<c32*>(smem_raw);
+  c32* const work = base + 2 * p.cap;
+  c32* const tab = base + 3 * p.cap;
+  const uint32_t tid = threadIdx.x;
+  uint32_t held0 = 0xFFFFFFFFu, held1 = 0xFFFFFFFFu;  // length whose tables slot 0/1 holds
+  bool tables = false;  // the slot being staged needs its tables (same in every thread)
+  // descriptors of task t into slot
+  auto stage = [&](uint32_t t, uint32_t slot) {
+    const LongTask task = p.tasks[t];
+    const LongLine ln = p.lines[task.line];
+    const uint32_t held = slot ? held1 : held0;
+    tables = ln.len != held;
+    if (tables) copy_words(&s_len[slot], p.lens + ln.len, tid, kLongThreads);
+    if (slot) held1 = ln.len;
+    else held0 = ln.len;
+    if (tid == 0) {
+      s_line[slot] = ln;
+      s_g0[slot] = task.g0;
+    }
+  };
+  auto issue = [&](uint32_t slot) {
+    const LongLenDesc& d = s_len[slot];
+    long_issue(p, d, s_line[slot], s_g0[slot], long_kind(p.phase, d.blue != 0), base + slot * p.cap,
+               tab + slot * kLongTab, tables, tid);
+  };
+  if (tid == 0) s_claim = atomicAdd(p.counter, 1u) * kLongChunk;
+  __syncthreads();
+  uint32_t t = s_claim;
+  uint32_t slot = 0;
+  if (t < p.ntasks) stage(t, 0);
+  __syncthreads();
+  if (t < p.ntasks) issue(0);
+  cp_async_commit();
+  while (t < p.ntasks) {
+    __syncthreads();  // every thread is past the previous task's stores and has read s_claim
+    uint32_t tn = t + 1;
+    if (tn % kLongChunk == 0 || tn >= p.ntasks) {  // next chunk
+      if (tid == 0) s_claim = atomicAdd(p.counter, 1u) * kLongChunk;
+      __syncthreads();
+      tn = s_claim;
+    }
+    if (tn < p.ntasks) stage(tn, slot ^ 1);
+    __syncthreads();
+    if (tn < p.ntasks) issue(slot ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();  // this thread's copies of the current task have landed
+    __syncthreads();
+    const LongLenDesc& d = s_len[slot];
+    long_compute(p, d, s_line[slot], s_g0[slot], long_kind(p.phase, d.blue != 0),
+                 base + slot * p.cap, work, tab + slot * kLongTab, tid);
+    slot ^= 1;
+    t = tn;
+  }
+  cp_async_wait<0>();
+}
+
+}  // namespace b2f
