@@ -10,10 +10,13 @@ flush is needed between steps).  One step = one batched launch over all
     execute_checked per line (what a caller of the reference's plan API does);
   - e2e: the batched step through the public API with the input copied from
     pinned host memory and the output copied back inside the timed region;
-  - roofline: the persistent CTA-queue kernel (k_batch_cta, every line with
-    the default routing), achieved algorithmic GB/s (16 B per complex point
-    per transform) against the measured HBM copy bandwidth, with the DRAM
-    traffic of an ncu capture (profiles/) scaled to the full launch;
+  - roofline: the long-line kernel (k_long_pass: the column, row and
+    Bluestein passes of every line too long for one CTA, which hold 97% of
+    the points), timed alone; achieved algorithmic GB/s (16 B per complex
+    point per transform, over the average of its launches of a step) against
+    the measured HBM copy bandwidth, with the DRAM traffic of an ncu capture
+    (profiles/) scaled to the full workload; the short-line CTA-queue kernel
+    (k_batch_cta) beside it;
   - serving: an open-loop Poisson request stream through the serving loop
     against the plain per-request path (p50/p99 latency, FFTs/s);
   - cpu_baseline: the planned CPU FFT (oracle/cpu_port.c, a C restatement of
@@ -425,52 +428,54 @@ def main():
     value = world * len(lengths) * args.steps / (total_ms / 1e3)
     clocks = clk.summary()
 
-    # ---- roofline of the dominant kernel.  With the default routing every
-    # line runs in k_batch_cta (one launch per step, after a 16-byte memset
-    # of the queue counters); its duration is timed on the launching stream.
+    # ---- roofline of the dominant kernel: k_long_pass (parts bit 2), its
+    # two or three launches of a step timed alone on the launching stream;
+    # the short-line kernel k_batch_cta (parts bit 0) beside it.
     hbm_peak, peak_kind = load_peaks()
     nd = diag
+    long_bytes = 16 * int(nd.get("long_elements", 0))
+    long_launches = max(1, int(nd.get("long_launches", 1)))
     cta_bytes = 16 * int(nd.get("cta_elements", 0))
-    cl_bytes = 16 * int(nd.get("cluster_elements", 0))
     rf = None
+
+    def time_parts(parts, reps):
+        for _ in range(2):
+            batch.execute_parts(dx, dy, parts, sequential=True)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(reps):
+            batch.execute_parts(dx, dy, parts, sequential=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / reps
+
     try:
         reps = max(3, args.steps)
-        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for _ in range(2):
-            batch.execute_parts(dx, dy, 1, sequential=True)
-        torch.cuda.synchronize()
-        k0.record(stream)
-        for _ in range(reps):
-            batch.execute_parts(dx, dy, 1, sequential=True)
-        k1.record(stream)
-        torch.cuda.synchronize()
-        cta_ms = k0.elapsed_time(k1) / reps
-        ach = cta_bytes / (cta_ms / 1e3) / 1e9
-        rf = {"bound": "hbm", "kernel": "k_batch_cta", "achieved": ach, "peak": hbm_peak,
+        long_ms = time_parts(4, reps)  # all launches of one step
+        per_launch_ms = long_ms / long_launches
+        per_launch_bytes = long_bytes / long_launches
+        ach = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+        rf = {"bound": "hbm", "kernel": "k_long_pass", "achieved": ach, "peak": hbm_peak,
               "unit": "GB/s", "frac": ach / hbm_peak, "peak_kind": peak_kind,
-              "traffic": None, "algorithmic_bytes_per_launch": cta_bytes,
-              "ms_per_launch": cta_ms,
+              "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes,
+              "ms_per_launch": per_launch_ms, "launches_per_step": long_launches,
               "whole_step": {"achieved": alg_bytes / (ms_per_step / 1e3) / 1e9,
                              "frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak}}
-        if cl_bytes:
-            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            batch.execute_parts(dx, dy, 2, sequential=True)
-            torch.cuda.synchronize()
-            c0.record(stream)
-            for _ in range(reps):
-                batch.execute_parts(dx, dy, 2, sequential=True)
-            c1.record(stream)
-            torch.cuda.synchronize()
-            cl_ms = c0.elapsed_time(c1) / reps
-            rf["other_kernel"] = {"kernel": "k_batch_cluster", "ms_per_launch": cl_ms,
-                                  "achieved": cl_bytes / (cl_ms / 1e3) / 1e9}
-        traffic_file = os.path.join(ROOT, "profiles", "k_batch_cta_traffic.json")
+        if cta_bytes:
+            cta_ms = time_parts(1, reps)
+            rf["other_kernel"] = {"kernel": "k_batch_cta", "ms_per_launch": cta_ms,
+                                  "algorithmic_bytes_per_launch": cta_bytes,
+                                  "achieved": cta_bytes / (cta_ms / 1e3) / 1e9}
+        traffic_file = os.path.join(ROOT, "profiles", "k_long_pass_traffic.json")
         if os.path.exists(traffic_file) and not args.lines:
             with open(traffic_file) as f:
                 t = json.load(f)
-            # DRAM bytes of one capture on a subset, scaled to the full launch by
-            # the algorithmic bytes (the traffic grows with the points processed)
-            rf["traffic"] = t["dram_bytes_per_launch"] * cta_bytes / t["algorithmic_bytes"]
+            # DRAM bytes of the launches of one step captured on a subset of the
+            # lines, per launch, scaled to the full workload by the algorithmic
+            # bytes (the traffic grows with the points processed)
+            rf["traffic"] = (t["dram_bytes_per_step"] / long_launches
+                             * long_bytes / t["algorithmic_bytes"])
             rf["traffic_note"] = t.get("note")
     except Exception as exc:  # measurement must not hide the headline
         rf = {"bound": "hbm", "error": str(exc)}
@@ -588,7 +593,9 @@ def main():
             "cpu_baseline": cpu,
             "accuracy": acc,
             "clocks": clocks,
-            "gpu_launches": args.steps * (int(diag.get("cta_launches", 1)) + int(diag["cluster_tasks"] > 0)
+            "gpu_launches": args.steps * (int(diag.get("cta_launches", 1))
+                                          + int(diag.get("long_launches", 0))
+                                          + int(diag["cluster_tasks"] > 0)
                                           + int(diag.get("cluster16_tasks", 0) > 0)),
             "batch": diag,
         }
