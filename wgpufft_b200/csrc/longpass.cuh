@@ -136,7 +136,7 @@ FFT_D void ilv_stage(const c32* __restrict__ src, c32* __restrict__ dst, const S
     k = s - fdiv(s, sd.dNs) * Ns;
     kinc = S - fdiv(S, sd.dNs) * Ns;
   }
-#pragma unroll 1
+#pragma unroll(R <= 8 ? 2 : 1)
   for (uint32_t j = s; j < NR; j += S) {
     const c32* sb = src + j * P + l;
     c32 v[R];
@@ -300,9 +300,22 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
   const LongSched& sch = colk ? d.s1 : d.s2;
   c32* r = X;
   c32* o = W;
-  // one FFT; the Bluestein middle pass runs two with the spectrum product
-  // (at k = k1 + N1 k2, k1 = g0 + l, k2 = i, conjugated) between them: the
-  // forward row FFT of the conjugate is the inverse row FFT
+  // the Bluestein middle pass multiplies by the chirp spectrum at
+  // k = k1 + N1 k2 (k1 = g0 + l, k2 = i0 + m S): its values are loaded into
+  // registers now, so the loads overlap the first FFT (m < ceil(N2 / S) <= 13
+  // for the row-task shapes: G = 16 up to 208 points, 8 up to 393, 4 up to 512)
+  constexpr int kBh = 13;
+  c32 bhv[kBh];
+  const uint32_t k1m = g0 + l;
+  if (kind == LP_BMID) {
+    const c32* bh = d.bhat + (k1m < N1 ? k1m : 0) + (uint64_t)N1 * i0;
+#pragma unroll
+    for (int m = 0; m < kBh; ++m)
+      bhv[m] = (i0 + m * S < N2) ? bh[(uint64_t)m * S * N1] : czero<float>();
+  }
+  // one FFT; the Bluestein middle pass runs two with the conjugated spectrum
+  // product between them: the forward row FFT of the conjugate is the
+  // inverse row FFT
   const int nfft = kind == LP_BMID ? 2 : 1;
 #pragma unroll 1
   for (int f = 0; f < nfft; ++f) {
@@ -310,17 +323,15 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
     o = (res == r) ? o : r;
     r = res;
     if (f + 1 == nfft) break;
-    const uint32_t k1 = g0 + l;
-    if (k1 < N1) {
+    if (k1m < N1) {
       c32* dp = r + i0 * P + l;
-      const c32* bh = d.bhat + k1 + (uint64_t)N1 * i0;
-#pragma unroll 4
-      for (uint32_t i = i0; i < N2; i += S) {
-        c32 v = cmul(*dp, *bh);
-        v.im = -v.im;
-        *dp = v;
-        dp += S * P;
-        bh += (uint64_t)S * N1;
+#pragma unroll
+      for (int m = 0; m < kBh; ++m) {
+        if (i0 + m * S < N2) {
+          c32 v = cmul(dp[m * S * P], bhv[m]);
+          v.im = -v.im;
+          dp[m * S * P] = v;
+        }
       }
     }
     __syncthreads();
