@@ -120,12 +120,49 @@ FFT_D c32 tw_two(const c32* __restrict__ tw, uint32_t ta, uint32_t tb, uint32_t 
   return cmul(tw[ta + a], tw[tb + b]);
 }
 
-// One radix-R stage over G interleaved lines, src -> dst: thread (l, s)
-// runs the butterflies j = s, s+S, ... of line l; k = j mod Ns advances by
-// S mod Ns.  tws: this stage's twiddles, row k at k*(R-1).
-template <int R>
+// Where the last stage of a pass puts its results: back into shared memory
+// (EpiNone), or straight from registers to global memory, value v of line l
+// at position pos: the column pass's scratch store with the inter-pass
+// twiddle (EpiCol), the row pass's output store (EpiRow).  A half-warp holds
+// one position of 16 lines, so each store is one G-value segment.
+struct EpiNone {
+  static constexpr bool active = false;
+  FFT_D void operator()(uint32_t, c32) const {}
+};
+struct EpiCol {  // scratch[N2 pos + c] = v * W_M^{c pos}
+  static constexpr bool active = true;
+  c32* dst;  // scratch of the line + c
+  const c32* T;
+  FastDiv dN2;
+  uint32_t N2, c;
+  bool ok;
+  FFT_D void operator()(uint32_t pos, c32 v) const {
+    if (ok) dst[(uint64_t)N2 * pos] = cmul(v, tw_two(T, kTabTa, kTabTb, c * pos, dN2));
+  }
+};
+struct EpiRow {  // out[k1 + N1 pos], scaled, conjugated back for inverse transforms
+  static constexpr bool active = true;
+  c32* dst;  // out of the line + k1
+  uint32_t N1;
+  float sc;
+  bool inv, ok;
+  FFT_D void operator()(uint32_t pos, c32 v) const {
+    if (ok) {
+      v.re *= sc;
+      v.im = inv ? -v.im * sc : v.im * sc;
+      dst[(uint64_t)N1 * pos] = v;
+    }
+  }
+};
+
+// One radix-R stage over G interleaved lines, src -> dst (or, for the last
+// stage with an active epilogue, src -> epi): thread (l, s) runs the
+// butterflies j = s, s+S, ... of line l; k = j mod Ns advances by S mod Ns.
+// tws: this stage's twiddles, row k at k*(R-1).
+template <int R, class Epi>
 FFT_D void ilv_stage(const c32* __restrict__ src, c32* __restrict__ dst, const StageDesc& sd,
-                     uint32_t lg, uint32_t tid, const c32* __restrict__ tws) {
+                     uint32_t lg, uint32_t tid, const c32* __restrict__ tws, bool to_epi,
+                     const Epi& epi) {
   const uint32_t G = 1u << lg, P = G + 1;
   const uint32_t l = tid & (G - 1), s = tid >> lg, S = kLongThreads >> lg;
   const uint32_t NR = sd.NR, Ns = sd.Ns;
@@ -148,38 +185,49 @@ FFT_D void ilv_stage(const c32* __restrict__ src, c32* __restrict__ dst, const S
       for (int q = 1; q < R; ++q) v[q] = cmul(v[q], t[q - 1]);
     }
     dft<float, R>(v);
-    c32* db = dst + ((j - k) * R + k) * P + l;
+    const uint32_t o = (j - k) * R + k;
+    if (Epi::active && to_epi) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) db[r * rs] = v[r];
+      for (int r = 0; r < R; ++r) epi(o + r * Ns, v[r]);
+    } else {
+      c32* db = dst + o * P + l;
+#pragma unroll
+      for (int r = 0; r < R; ++r) db[r * rs] = v[r];
+    }
     k += kinc;
     if (k >= Ns) k -= Ns;
   }
 }
 
-// The whole schedule, a <-> b; returns the buffer holding the result.  T:
-// the table area (stage twiddles from offset kTabSt, global table offsets
-// relative to the first stage's).  The caller synchronises before; every
-// stage ends with a barrier.
-FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t tid,
-                   const c32* T) {
+// The whole schedule, a <-> b; returns the buffer holding the result (with
+// an active epilogue the last stage goes to epi and the return value is
+// meaningless).  T: the table area (stage twiddles from offset kTabSt,
+// global table offsets relative to the first stage's).  The caller
+// synchronises before; every stage that writes shared memory ends with a
+// barrier.
+template <class Epi>
+FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t tid, const c32* T,
+                   const Epi& epi) {
   const uint32_t tw0 = sch.st[0].tw_off;
 #pragma unroll 1
   for (uint32_t s = 0; s < sch.nst; ++s) {
     const StageDesc& sd = sch.st[s];
     const c32* tws = T + kTabSt + (sd.tw_off - tw0);
+    const bool to_epi = Epi::active && s + 1 == sch.nst;
     switch (sd.R) {
-      case 2: ilv_stage<2>(a, b, sd, lg, tid, tws); break;
-      case 3: ilv_stage<3>(a, b, sd, lg, tid, tws); break;
-      case 4: ilv_stage<4>(a, b, sd, lg, tid, tws); break;
-      case 5: ilv_stage<5>(a, b, sd, lg, tid, tws); break;
-      case 7: ilv_stage<7>(a, b, sd, lg, tid, tws); break;
-      case 8: ilv_stage<8>(a, b, sd, lg, tid, tws); break;
-      case 9: ilv_stage<9>(a, b, sd, lg, tid, tws); break;
-      case 11: ilv_stage<11>(a, b, sd, lg, tid, tws); break;
-      case 13: ilv_stage<13>(a, b, sd, lg, tid, tws); break;
-      case 16: ilv_stage<16>(a, b, sd, lg, tid, tws); break;
+      case 2: ilv_stage<2>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 3: ilv_stage<3>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 4: ilv_stage<4>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 5: ilv_stage<5>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 7: ilv_stage<7>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 8: ilv_stage<8>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 9: ilv_stage<9>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 11: ilv_stage<11>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 13: ilv_stage<13>(a, b, sd, lg, tid, tws, to_epi, epi); break;
+      case 16: ilv_stage<16>(a, b, sd, lg, tid, tws, to_epi, epi); break;
       default: break;
     }
+    if (to_epi) break;
     __syncthreads();
     c32* t = a;
     a = b;
@@ -298,6 +346,29 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
     __syncthreads();
   }
   const LongSched& sch = colk ? d.s1 : d.s2;
+  if (kind == LP_COL || kind == LP_BCOL1) {
+    // scratch[k1][g0 + l] = X[k1] * W_M^{(g0+l) k1}, from the last stage
+    EpiCol e;
+    e.c = g0 + l;
+    e.ok = e.c < N2;
+    e.dst = p.scratch + ln.scratch + (e.ok ? e.c : 0);
+    e.T = T;
+    e.dN2 = d.dN2;
+    e.N2 = N2;
+    ilv_fft(X, W, sch, lg, tid, T, e);
+    return;
+  }
+  if (kind == LP_ROW) {
+    // out[k1 + N1 k2], k1 = g0 + l, from the last stage
+    EpiRow e;
+    e.ok = g0 + l < N1;
+    e.dst = p.out + ln.base + (e.ok ? g0 + l : 0);
+    e.N1 = N1;
+    e.sc = d.scale;
+    e.inv = inv;
+    ilv_fft(X, W, sch, lg, tid, T, e);
+    return;
+  }
   c32* r = X;
   c32* o = W;
   // the Bluestein middle pass multiplies by the chirp spectrum at
@@ -319,7 +390,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
   const int nfft = kind == LP_BMID ? 2 : 1;
 #pragma unroll 1
   for (int f = 0; f < nfft; ++f) {
-    c32* res = ilv_fft(r, o, sch, lg, tid, T);
+    c32* res = ilv_fft(r, o, sch, lg, tid, T, EpiNone());
     o = (res == r) ? o : r;
     r = res;
     if (f + 1 == nfft) break;
@@ -337,37 +408,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
     __syncthreads();
   }
   // stores
-  if (kind == LP_COL || kind == LP_BCOL1) {
-    // scratch[k1][g0 + l] = X[k1] * W_M^{(g0+l) k1}
-    const uint32_t c = g0 + l;
-    if (c < N2) {
-      c32* dst = p.scratch + ln.scratch + (uint64_t)N2 * i0 + c;
-      const c32* sp = r + i0 * P + l;
-#pragma unroll 4
-      for (uint32_t k1 = i0; k1 < N1; k1 += S) {
-        *dst = cmul(*sp, tw_two(T, kTabTa, kTabTb, c * k1, d.dN2));
-        dst += (uint64_t)S * N2;
-        sp += S * P;
-      }
-    }
-  } else if (kind == LP_ROW) {
-    // out[k1 + N1 k2], k1 = g0 + l
-    const uint32_t k1 = g0 + l;
-    if (k1 < N1) {
-      const float sc = d.scale;
-      c32* dst = p.out + ln.base + k1 + (uint64_t)N1 * i0;
-      const c32* sp = r + i0 * P + l;
-#pragma unroll 4
-      for (uint32_t k2 = i0; k2 < N2; k2 += S) {
-        c32 v = *sp;
-        v.re *= sc;
-        v.im = inv ? -v.im * sc : v.im * sc;
-        *dst = v;
-        dst += (uint64_t)S * N1;
-        sp += S * P;
-      }
-    }
-  } else if (kind == LP_BMID) {
+  if (kind == LP_BMID) {
     // scratch row k1 = g0 + r, position n2: V * W_M^{n2 k1} (warp w writes rows w, w+8, ...)
     const uint32_t w = tid >> 5, lane = tid & 31;
     for (uint32_t rr = w; rr < G; rr += kLongThreads / 32) {
