@@ -56,6 +56,12 @@ typedef int32_t b2f_status;
 #define B2F_ERR_INVALID_ARGUMENT 15        /* null handle or pointer (Rust references cannot be null) */
 #define B2F_ERR_DEVICE 16                  /* a CUDA call failed (wgpu validation/device error) */
 #define B2F_ERR_WORKSPACE_TOO_SMALL 17     /* FftError::WorkspaceTooSmall */
+/* Tuning-snapshot decoding, the four variants of the crate's
+ * PipelineCacheSnapshotError (src/runtime/pipeline_cache.rs:58-74). */
+#define B2F_ERR_SNAPSHOT_JSON 18           /* PipelineCacheSnapshotError::Json */
+#define B2F_ERR_SNAPSHOT_SCHEMA 19         /* PipelineCacheSnapshotError::SchemaMismatch */
+#define B2F_ERR_SNAPSHOT_VERSION 20        /* PipelineCacheSnapshotError::VersionMismatch */
+#define B2F_ERR_SNAPSHOT_INTEGRITY 21      /* PipelineCacheSnapshotError::Integrity */
 
 /* FftDirection (src/config.rs:43-57). */
 #define B2F_FORWARD 0
@@ -107,6 +113,8 @@ b2f_status b2f_config_set_precision(b2f_config* cfg, int32_t precision);
 b2f_status b2f_config_set_tuning(b2f_config* cfg, const char* key, int64_t value);
 /* FftTuning::with_force_rader_axes / with_force_bluestein_axes
  * (src/tuning.rs:197-205): key "force_rader_axes" or "force_bluestein_axes". */
+/* Reads back one scalar FftTuning field (same keys as b2f_config_set_tuning). */
+b2f_status b2f_config_get_tuning(const b2f_config* cfg, const char* key, int64_t* value);
 b2f_status b2f_config_set_tuning_axes(b2f_config* cfg, const char* key, const uint32_t* axes,
                                       uint32_t count);
 /* FftConfig::validate (src/config.rs:178-211). */
@@ -263,6 +271,42 @@ b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint64_t in_byte
 /* --------------------------------------------------------------- errors */
 
 /* FftError's Display (src/error.rs): a fixed name for each status. */
+/* ------------------------------------------- autotuner and tuning snapshot */
+
+/* Autotuner (the batching form's "autotuner + tuning snapshot"; nearest
+ * reference ancestors: FftTuning, src/tuning.rs:35-268, and the pipeline
+ * cache snapshot, src/runtime/pipeline_cache.rs:14-395).  Creates the plan of
+ * `cfg` (kind B2F_C2C/R2C/C2R) on `device`, times it and candidate tunings
+ * of the kernel-shape knobs (twiddle_table, then lines_per_block 1..16, then
+ * threads_per_block 64..512; `reps` executions each after two warm-ups, 0 =
+ * 20) on buffers it allocates and fills with deterministic values, keeps the
+ * fastest candidate whose output matches the default plan's within the
+ * precision's tolerance (f32 2e-6, f64 1e-13, df64 1e-12 relative L2), and
+ * records it in the process-wide tuning snapshot.  The report (JSON: key,
+ * default_us, best_us, best, every candidate with its time and error) is
+ * written to report as b2f_plan_diagnostics_json does. */
+b2f_status b2f_autotune(const b2f_config* cfg, int32_t kind, int32_t device, uint32_t reps,
+                        char* report, uint64_t* len);
+/* Records a tuning for cfg's key by hand (validated like a plan's tuning). */
+b2f_status b2f_tuning_snapshot_record(const b2f_config* cfg, int32_t kind, int64_t lines_per_block,
+                                      int64_t threads_per_block, int64_t twiddle_table,
+                                      double best_us, double default_us);
+/* Copies the snapshot's tuning for cfg's key into cfg; *found = 0 or 1. */
+b2f_status b2f_tuning_snapshot_apply(b2f_config* cfg, int32_t kind, int32_t* found);
+/* The snapshot as versioned JSON (schema "wgpufft_b200.tuning", version 1,
+ * device, entries ordered by key, FNV-1a checksum over device and entries). */
+b2f_status b2f_tuning_snapshot_json(char* buf, uint64_t* len);
+b2f_status b2f_tuning_snapshot_save(const char* path);
+/* Replaces the snapshot with the file's after checking it: JSON syntax and
+ * fields (SnapshotJson), schema (SnapshotSchemaMismatch), version
+ * (SnapshotVersionMismatch), and integrity (SnapshotIntegrity): every key
+ * canonical and re-derived from its fields, keys strictly ordered (no
+ * duplicates), tuning values valid for their configuration, checksum, and,
+ * with device >= 0, entries measured on a device of the same name and
+ * architecture.  On any error the snapshot in memory is unchanged. */
+b2f_status b2f_tuning_snapshot_load(const char* path, int32_t device);
+void b2f_tuning_snapshot_clear(void);
+
 const char* b2f_status_string(b2f_status status);
 /* Detail of the calling thread's last failure; returns its length and
  * copies at most len-1 bytes plus a NUL into buf (buf may be NULL). */

@@ -66,6 +66,15 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_config_set_normalization": (st, [vp, i32]),
         "b2f_config_set_precision": (st, [vp, i32]),
         "b2f_config_set_tuning": (st, [vp, ctypes.c_char_p, ctypes.c_int64]),
+        "b2f_config_get_tuning": (st, [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
+        "b2f_autotune": (st, [vp, i32, i32, u32, ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_tuning_snapshot_record": (st, [vp, i32, ctypes.c_int64, ctypes.c_int64,
+                                            ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
+        "b2f_tuning_snapshot_apply": (st, [vp, i32, ctypes.POINTER(i32)]),
+        "b2f_tuning_snapshot_json": (st, [ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_tuning_snapshot_save": (st, [ctypes.c_char_p]),
+        "b2f_tuning_snapshot_load": (st, [ctypes.c_char_p, i32]),
+        "b2f_tuning_snapshot_clear": (None, []),
         "b2f_config_set_tuning_axes": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u32), u32]),
         "b2f_config_validate": (st, [vp]),
         "b2f_config_required_buffer_size_bytes": (st, [vp, ctypes.POINTER(u64)]),
@@ -631,6 +640,73 @@ class FftServer:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------- autotuner and snapshot
+def _json_out(fn, *args) -> str:
+    n = ctypes.c_uint64(0)
+    _check(fn(*args, None, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    n2 = ctypes.c_uint64(n.value + 1)
+    _check(fn(*args, buf, ctypes.byref(n2)))
+    return buf.value.decode()
+
+
+def autotune(config: FftConfig, kind: FftTransformKind = FftTransformKind.C2c,
+             device: Optional[int] = None, reps: int = 20) -> dict:
+    """Times candidate tunings of `config` on the device (b2f_autotune),
+    records the fastest one that matches the default plan's results in the
+    process-wide tuning snapshot and returns the report."""
+    with _ConfigHandle(config) as h:
+        dev = -1 if device is None else int(device)
+        return json.loads(_json_out(lib().b2f_autotune, h.ptr, int(kind), dev, int(reps)))
+
+
+def tuned_config(config: FftConfig, kind: FftTransformKind = FftTransformKind.C2c):
+    """(config with the snapshot's tuning for its key applied, found)."""
+    L = lib()
+    with _ConfigHandle(config) as h:
+        found = ctypes.c_int32(0)
+        _check(L.b2f_tuning_snapshot_apply(h.ptr, int(kind), ctypes.byref(found)))
+        if not found.value:
+            return config, False
+        vals = {}
+        for k in ("lines_per_block", "threads_per_block", "twiddle_table"):
+            v = ctypes.c_int64(0)
+            _check(L.b2f_config_get_tuning(h.ptr, k.encode(), ctypes.byref(v)))
+            vals[k] = int(v.value)
+    t = config._tuning
+    t = t.with_lines_per_block(vals["lines_per_block"]).with_threads_per_block(
+        vals["threads_per_block"]).with_twiddle_table(bool(vals["twiddle_table"]))
+    return config.with_tuning(t), True
+
+
+def tuning_snapshot_record(config: FftConfig, kind: FftTransformKind, lines_per_block: int,
+                           threads_per_block: int, twiddle_table: int, best_us: float = 0.0,
+                           default_us: float = 0.0) -> None:
+    with _ConfigHandle(config) as h:
+        _check(lib().b2f_tuning_snapshot_record(h.ptr, int(kind), lines_per_block,
+                                                threads_per_block, twiddle_table, best_us,
+                                                default_us))
+
+
+def tuning_snapshot_json() -> dict:
+    return json.loads(_json_out(lib().b2f_tuning_snapshot_json))
+
+
+def tuning_snapshot_save(path: str) -> None:
+    _check(lib().b2f_tuning_snapshot_save(os.fsencode(path)))
+
+
+def tuning_snapshot_load(path: str, device: Optional[int] = None) -> None:
+    """Loads a snapshot file after its schema, version, integrity and (with a
+    device) device checks; raises FftError and keeps the current snapshot
+    otherwise."""
+    _check(lib().b2f_tuning_snapshot_load(os.fsencode(path), -1 if device is None else int(device)))
+
+
+def tuning_snapshot_clear() -> None:
+    lib().b2f_tuning_snapshot_clear()
 
 
 def _host_buf(b) -> Tuple[int, int]:

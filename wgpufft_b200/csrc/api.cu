@@ -71,29 +71,41 @@ b2f_status b2f_config_set_precision(b2f_config* cfg, int32_t precision) {
   return B2F_OK;
 }
 
+static int64_t* tuning_field(Tuning& t, const std::string& k) {
+  if (k == "workgroup_size") return &t.workgroup_size;
+  if (k == "fused_workgroup_size") return &t.fused_workgroup_size;
+  if (k == "rader_max_prime") return &t.rader_max_prime;
+  if (k == "direct_max_prime") return &t.direct_max_prime;
+  if (k == "large_route") return &t.large_route;
+  if (k == "large_chunk_max_batches") return &t.large_chunk_max_batches;
+  if (k == "grouped_batch") return &t.grouped_batch;
+  if (k == "swap_to_2_stage_4_step") return &t.swap_to_2_stage_4_step;
+  if (k == "swap_to_3_stage_4_step") return &t.swap_to_3_stage_4_step;
+  if (k == "segmented_burst_depth") return &t.segmented_burst_depth;
+  if (k == "max_storage_buffer_binding_size") return &t.max_storage_buffer_binding_size;
+  if (k == "max_buffer_size") return &t.max_buffer_size;
+  if (k == "fused_min_convolution_length") return &t.fused_min_convolution_length;
+  if (k == "fuse_long_axes") return &t.fuse_long_axes;
+  if (k == "fuse_small_volumes") return &t.fuse_small_volumes;
+  if (k == "lines_per_block") return &t.lines_per_block;
+  if (k == "threads_per_block") return &t.threads_per_block;
+  if (k == "twiddle_table") return &t.twiddle_table;
+  return nullptr;
+}
+
 b2f_status b2f_config_set_tuning(b2f_config* cfg, const char* key, int64_t value) {
   REQUIRE(cfg && key, "null config or key");
-  Tuning& t = cfg->cfg.tuning;
-  const std::string k(key);
-  if (k == "workgroup_size") t.workgroup_size = value;
-  else if (k == "fused_workgroup_size") t.fused_workgroup_size = value;
-  else if (k == "rader_max_prime") t.rader_max_prime = value;
-  else if (k == "direct_max_prime") t.direct_max_prime = value;
-  else if (k == "large_route") t.large_route = value;
-  else if (k == "large_chunk_max_batches") t.large_chunk_max_batches = value;
-  else if (k == "grouped_batch") t.grouped_batch = value;
-  else if (k == "swap_to_2_stage_4_step") t.swap_to_2_stage_4_step = value;
-  else if (k == "swap_to_3_stage_4_step") t.swap_to_3_stage_4_step = value;
-  else if (k == "segmented_burst_depth") t.segmented_burst_depth = value;
-  else if (k == "max_storage_buffer_binding_size") t.max_storage_buffer_binding_size = value;
-  else if (k == "max_buffer_size") t.max_buffer_size = value;
-  else if (k == "fused_min_convolution_length") t.fused_min_convolution_length = value;
-  else if (k == "fuse_long_axes") t.fuse_long_axes = value;
-  else if (k == "fuse_small_volumes") t.fuse_small_volumes = value;
-  else if (k == "lines_per_block") t.lines_per_block = value;
-  else if (k == "threads_per_block") t.threads_per_block = value;
-  else if (k == "twiddle_table") t.twiddle_table = value;
-  else return fail(B2F_ERR_INVALID_ARGUMENT, "unknown tuning key: " + k);
+  int64_t* f = tuning_field(cfg->cfg.tuning, key);
+  if (!f) return fail(B2F_ERR_INVALID_ARGUMENT, std::string("unknown tuning key: ") + key);
+  *f = value;
+  return B2F_OK;
+}
+
+b2f_status b2f_config_get_tuning(const b2f_config* cfg, const char* key, int64_t* value) {
+  REQUIRE(cfg && key && value, "null config, key or output");
+  int64_t* f = tuning_field(const_cast<b2f_config*>(cfg)->cfg.tuning, key);
+  if (!f) return fail(B2F_ERR_INVALID_ARGUMENT, std::string("unknown tuning key: ") + key);
+  *value = *f;
   return B2F_OK;
 }
 
@@ -307,6 +319,10 @@ const char* b2f_status_string(b2f_status s) {
     case B2F_ERR_INVALID_ARGUMENT: return "InvalidArgument";
     case B2F_ERR_DEVICE: return "DeviceError";
     case B2F_ERR_WORKSPACE_TOO_SMALL: return "WorkspaceTooSmall";
+    case B2F_ERR_SNAPSHOT_JSON: return "SnapshotJson";
+    case B2F_ERR_SNAPSHOT_SCHEMA: return "SnapshotSchemaMismatch";
+    case B2F_ERR_SNAPSHOT_VERSION: return "SnapshotVersionMismatch";
+    case B2F_ERR_SNAPSHOT_INTEGRITY: return "SnapshotIntegrity";
     default: return "Unknown";
   }
 }
