@@ -173,3 +173,17 @@ def test_execute_on_plan_only_plan_fails_loudly():
     with pytest.raises(w.FftError) as e:
         p.execute_checked((0x1000, 128), (0x2000, 128))
     assert e.value.kind == "DeviceError"
+
+
+def test_tensor_core_knob_routes_and_validates():
+    tc = w.FftTuning().with_tensor_cores(True)
+    d = plan_only(w.FftConfig.new(64).with_batch(1000).with_tuning(tc)).diagnostics()
+    assert [s["kind"] for s in d["stages"]] == ["tensor-core-dft"]
+    # only length-64 f32 lines of axis 0 take the tensor-core layer
+    for cfg in (w.FftConfig.new(128).with_tuning(tc),
+                w.FftConfig.new(64).with_precision(w.FftPrecision.F64).with_tuning(tc),
+                w.FftConfig.new_nd([32, 64]).with_tuning(tc)):
+        assert all(s["kind"] != "tensor-core-dft" for s in plan_only(cfg).diagnostics()["stages"])
+    with pytest.raises(w.FftError) as e:
+        w.FftConfig.new(64).with_tuning(w.FftTuning().with_tensor_cores(2)).validate()
+    assert e.value.kind == "InvalidTuning"

@@ -185,7 +185,7 @@ _SCALAR_TUNING = (
     "large_route", "large_chunk_max_batches", "grouped_batch", "swap_to_2_stage_4_step",
     "swap_to_3_stage_4_step", "segmented_burst_depth", "max_storage_buffer_binding_size",
     "max_buffer_size", "fused_min_convolution_length", "fuse_long_axes", "fuse_small_volumes",
-    "lines_per_block", "threads_per_block", "twiddle_table",
+    "lines_per_block", "threads_per_block", "twiddle_table", "tensor_cores",
 )
 _TUNING_DEFAULTS = {
     "workgroup_size": 64, "fused_workgroup_size": 256, "rader_max_prime": 8192,
@@ -194,7 +194,7 @@ _TUNING_DEFAULTS = {
     "segmented_burst_depth": 2, "max_storage_buffer_binding_size": None,
     "max_buffer_size": None, "fused_min_convolution_length": 128, "fuse_long_axes": True,
     "fuse_small_volumes": True, "lines_per_block": 0, "threads_per_block": 0,
-    "twiddle_table": True,
+    "twiddle_table": True, "tensor_cores": False,
 }
 
 

@@ -241,6 +241,8 @@ static b2f_status validate_tuning(const Config& cfg) {
     return invalid_tuning("swap_to_2_stage_4_step", t.swap_to_2_stage_4_step,
                           "ConflictingValues",
                           "must not exceed swap_to_3_stage_4_step when both thresholds are active");
+  if (t.tensor_cores != 0 && t.tensor_cores != 1)
+    return invalid_tuning("tensor_cores", t.tensor_cores, "InvalidValue", "must be 0 or 1");
   if (t.lines_per_block < 0)
     return invalid_tuning("lines_per_block", t.lines_per_block, "InvalidValue",
                           "must be zero (planner's choice) or positive");
@@ -1045,7 +1047,8 @@ static void build_diagnostics(Plan& plan) {
     const char* kind = p.kind == Pass::LINES ? "lines" : p.kind == Pass::POW2 ? (p.colmajor ? "register-pow2-columns" : "register-pow2-lines") : p.kind == Pass::RADER ? "rader"
                      : p.kind == Pass::BLUESTEIN ? "bluestein" : p.kind == Pass::R2C ? "r2c"
                      : p.kind == Pass::C2R ? "c2r" : p.kind == Pass::BLUE_ELEM ? "bluestein-elementwise"
-                     : p.kind == Pass::REAL_ELEM ? "real-elementwise" : "scale-copy";
+                     : p.kind == Pass::REAL_ELEM ? "real-elementwise"
+                     : p.kind == Pass::TC_DFT64 ? "tensor-core-dft" : "scale-copy";
     uint32_t G = (p.kind == Pass::LINES || p.kind == Pass::POW2) ? p.lines.G : p.kind == Pass::RADER ? p.rader.L.G
                : p.kind == Pass::BLUESTEIN ? p.blue.L.G : (p.kind == Pass::R2C || p.kind == Pass::C2R) ? p.real.G : 0;
     os << (i ? "," : "") << "{\"label\":\"" << json_escape(p.label) << "\",\"kind\":\"" << kind
@@ -1077,7 +1080,8 @@ static void build_diagnostics(Plan& plan) {
      << ",\"fuse_long_axes\":" << (t.fuse_long_axes ? "true" : "false")
      << ",\"fuse_small_volumes\":" << (t.fuse_small_volumes ? "true" : "false")
      << ",\"lines_per_block\":" << t.lines_per_block << ",\"threads_per_block\":" << t.threads_per_block
-     << ",\"twiddle_table\":" << (t.twiddle_table ? "true" : "false") << "}";
+     << ",\"twiddle_table\":" << (t.twiddle_table ? "true" : "false")
+     << ",\"tensor_cores\":" << (t.tensor_cores ? "true" : "false") << "}";
   os << ",\"tuning\":{\"requested\":" << tj.str() << ",\"effective\":" << tj.str() << "}";
   os << ",\"supports_in_place\":" << (plan.in_place_kernels ? "true" : "false");
   os << ",\"device\":" << plan.device << "}";
@@ -1150,6 +1154,31 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
       ps.dst = BUF_OUT;
       ps.copy_n = 1;
       ps.copy_scale = scale;
+      plan->passes.push_back(ps);
+    } else if (cfg.tuning.tensor_cores && plan->prec == PREC_F32 && cfg.axes.size() == 1 &&
+               cfg.axes[0] == 0 && cfg.shape[0] == 64) {
+      // the tensor-core DFT layer: every (contiguous) line of axis 0 in one pass
+      Pass ps;
+      ps.kind = Pass::TC_DFT64;
+      ps.label = "tensor-core-dft64-split-tf32-stage";
+      ps.route = "mixed-radix";
+      ps.axis = 0;
+      ps.src = BUF_IN;
+      ps.dst = BUF_OUT;
+      ps.radices = {64};
+      ps.tc_nlines = total / 64;
+      ps.tc_scale = (float)scale;
+      ps.tc_inverse = inverse;
+      ps.threads = 256;
+      ps.smem = 192 * 1024;
+      int nsm = 148;
+      if (!dry) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+      ps.grid = (unsigned)std::min<uint64_t>((uint64_t)nsm, (ps.tc_nlines + 63) / 64);
+      const std::vector<float> tab = dft64_tc_table();
+      std::vector<unsigned char> tb(tab.size() * 4);
+      std::memcpy(tb.data(), tab.data(), tb.size());
+      ps.tc_table = b.add_table(std::move(tb));
+      ps.tc_err = b.add_table(std::vector<unsigned char>(16, 0));
       plan->passes.push_back(ps);
     } else {
       for (size_t ai = 0; ai < cfg.axes.size(); ++ai) {
@@ -1296,6 +1325,11 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
         p.relem.in = src;
         p.relem.out = dst;
         e = launch_real_elem(plan.prec, p.relem, st);
+        break;
+      case Pass::TC_DFT64:
+        e = launch_dft64_tc(src, dst, (const float*)plan.device_allocs[p.tc_table], p.tc_nlines,
+                            p.tc_scale, p.tc_inverse, (unsigned int*)plan.device_allocs[p.tc_err],
+                            p.grid, st);
         break;
     }
     if (e != cudaSuccess) break;

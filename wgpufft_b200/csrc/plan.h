@@ -36,6 +36,7 @@ struct Tuning {
   int64_t lines_per_block = 0;
   int64_t threads_per_block = 0;
   int64_t twiddle_table = 1;
+  int64_t tensor_cores = 0;  // 1: length-64 f32 lines on the tcgen05 split-TF32 DFT layer
 };
 
 struct Config {
@@ -58,7 +59,7 @@ enum BufId : int {
 constexpr int kNumWorkspaces = 6;
 
 struct Pass {
-  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM, REAL_ELEM } kind = LINES;
+  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM, REAL_ELEM, TC_DFT64 } kind = LINES;
   int pow2_E = 16;         // POW2: values per thread
   bool colmajor = false;   // POW2: adjacent lines first
   std::string label;  // stage label (diagnostics)
@@ -77,6 +78,12 @@ struct Pass {
   uint64_t copy_n = 0;
   double copy_scale = 1.0;
   bool copy_conj = false;
+  // TC_DFT64: lines, their scale and direction, device_allocs indices of the
+  // operand table and of the wait-timeout flag
+  uint64_t tc_nlines = 0;
+  float tc_scale = 1.0f;
+  bool tc_inverse = false;
+  size_t tc_table = 0, tc_err = 0;
 };
 
 struct Plan {
@@ -107,6 +114,11 @@ struct Plan {
 };
 
 b2f_status validate_config(const Config& cfg);
+// Tensor-core DFT layer (tc_dft.cu): the split operand table and the launcher.
+std::vector<float> dft64_tc_table();
+cudaError_t launch_dft64_tc(const void* in, void* out, const float* table, uint64_t nlines,
+                            float scale, bool inverse, unsigned int* err, unsigned grid,
+                            cudaStream_t st);
 b2f_status create_plan(const Config& cfg, int32_t kind, int device, Plan** out);
 b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint64_t in_bytes,
                         void* out, uint64_t out_bytes);
