@@ -261,6 +261,11 @@ def config_measurements(local, hbm_peak):
          False, False),
         ("1d_2^20x16_df64", w.FftConfig.new(1 << 20).with_batch(16).with_precision(DF64), C2C,
          False, False),
+        # the precision form: 2^20 lines of 64 on the tcgen05 split-TF32 layer, beside the
+        # same lines on the CUDA-core register kernel
+        ("1d_64x2^20_tensor_cores", w.FftConfig.new(64).with_batch(1 << 20).with_tuning(
+            w.FftTuning().with_tensor_cores(True)), C2C, False, False),
+        ("1d_64x2^20", w.FftConfig.new(64).with_batch(1 << 20), C2C, False, False),
     ]
     out = {}
     stream = torch.cuda.current_stream()

@@ -1173,7 +1173,7 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
       ps.smem = 192 * 1024;
       int nsm = 148;
       if (!dry) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-      ps.grid = (unsigned)std::min<uint64_t>((uint64_t)nsm, (ps.tc_nlines + 63) / 64);
+      ps.grid = (unsigned)std::min<uint64_t>((uint64_t)nsm, (ps.tc_nlines + 31) / 32);
       const std::vector<float> tab = dft64_tc_table();
       std::vector<unsigned char> tb(tab.size() * 4);
       std::memcpy(tb.data(), tab.data(), tb.size());

@@ -1,13 +1,13 @@
 // Tensor-core DFT layer (the precision form): batched length-64 complex
-// DFTs as one real GEMM on the 5th-generation tensor cores (tcgen05), in
-// f32 accuracy from split TF32 operands.
+// DFTs as real GEMMs on the 5th-generation tensor cores (tcgen05), in f32
+// accuracy from split TF32 operands.
 //
 // The complex DFT y = F x of a line is the real product
 //   [yr; yi] = A [xr; xi],  A = [[C, S], [-S, C]],  C = cos(2 pi r m / 64),
 //   S = sin(2 pi r m / 64)                                   (128 x 128),
-// so a tile of 64 lines is D (128 x 64) = A (128 x 128) * B^T with B the
-// 64 x 128 matrix of the lines' [re; im] values: one tcgen05.mma M = 128,
-// N = 64 per K-step of 8.  Each operand is split into a TF32 high part (low
+// so a tile of 32 lines is D (128 x 32) = A (128 x 128) * B^T with B the
+// 32 x 128 matrix of the lines' [re; im] values: tcgen05.mma with M = 128,
+// N = 32 per K-step of 8.  Each operand is split into a TF32 high part (low
 // 13 bits cleared: exact) and the remainder, and three products
 //   D = Ah Bh + Ah Bl + Al Bh
 // accumulate in FP32 in tensor memory: the dropped Al Bl term and the
@@ -18,13 +18,13 @@
 //
 // Operands sit in shared memory in the K-major, no-swizzle canonical
 // layout: 8-row x 16-byte core matrices, consecutive along K (LBO = 128 B),
-// row groups 4096 B apart (SBO).  One elected thread issues the 48 MMAs and
-// commits them to an mbarrier; the CTA waits on it (bounded: past the limit
-// it records an error and carries on), reads the accumulator with
-// tcgen05.ld (warp w holds rows 32w..32w+31), transposes through shared
-// memory and stores coalesced (two warpgroups: warp w reads TMEM lanes
-// 32 (w % 4).. and half the columns).  TMEM: 64 columns, allocated once per
-// CTA and freed before exit.
+// row groups 4096 B apart (SBO).  One thread issues a tile's 48 MMAs and
+// commits them to the tile's mbarrier; waits on it are bounded (past the
+// limit the kernel records an error, waits once more and stops).  The
+// accumulator is read with tcgen05.ld (warp w: TMEM lanes 32 (w % 4).., one
+// half of the lines per warpgroup), transposed through shared memory and
+// stored coalesced.  The kernel is persistent and software-pipelined over
+// two operand buffers, two 32-column accumulators and two mbarriers.
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -36,13 +36,14 @@ namespace b2f {
 
 namespace {
 
-constexpr uint32_t kTcR = 64, kTcM = 128, kTcK = 128, kTcN = 64;
+constexpr uint32_t kTcR = 64, kTcM = 128, kTcK = 128, kTcN = 32;  // N: lines per tile
 constexpr uint32_t kTcKC = kTcK / 4;                  // 16-byte chunks along K
 constexpr uint32_t kTcABytes = kTcM * kTcK * 4;       // one split half of A: 64 KB
-constexpr uint32_t kTcBBytes = kTcN * kTcK * 4;       // one split half of a B tile: 32 KB
-constexpr uint32_t kTcSmem = 2 * kTcABytes + 2 * kTcBBytes;  // 192 KB
+constexpr uint32_t kTcBBytes = kTcN * kTcK * 4;       // one split half of a B tile: 16 KB
+constexpr uint32_t kTcSmem = 2 * kTcABytes + 4 * kTcBBytes;  // A halves + two B buffers: 192 KB
 constexpr uint32_t kTcWaitLimit = 1u << 26;           // mbarrier polls before giving up
 constexpr uint32_t kTcThreads = 256;                  // two warpgroups
+constexpr uint32_t kTcPer = kTcN * kTcR / kTcThreads;   // complex values per thread and tile
 
 __host__ __device__ inline uint32_t tc_off(uint32_t row, uint32_t k) {
   return (((row >> 3) * kTcKC + (k >> 2)) << 7) + ((row & 7) << 4) + ((k & 3) << 2);
@@ -60,7 +61,7 @@ __device__ inline uint64_t tc_desc(uint32_t saddr) {
   return d;                                              // base offset 0, no swizzle
 }
 
-// kind::tf32, D in F32, A and B K-major, M = 128, N = 64
+// kind::tf32, D in F32, A and B K-major, M = 128, N = 32
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((kTcN >> 3) << 17) |
                               ((kTcM >> 4) << 24);
 
@@ -111,34 +112,75 @@ __device__ inline bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+// Element j of thread tid within a tile: each group of 32 consecutive
+// elements (a warp's) covers 8 lines x 4 consecutive positions, so the
+// split stores of a warp hit 32 different banks (a core-matrix row is 16
+// bytes of one line, rows of 8 lines are consecutive).
+__device__ inline void tc_elem(uint32_t tid, uint32_t j, uint32_t& n, uint32_t& m) {
+  const uint32_t e = tid + j * kTcThreads, g = e >> 5, lane = e & 31;
+  n = (g & (kTcN / 8 - 1)) * 8 + (lane >> 2);
+  m = (g / (kTcN / 8)) * 4 + (lane & 3);
+}
+
+// Loads of one tile into registers.
+__device__ inline void tc_load(const float2* __restrict__ in, uint64_t line0, uint64_t nlines,
+                               uint32_t tid, float2* reg) {
+#pragma unroll
+  for (uint32_t j = 0; j < kTcPer; ++j) {
+    uint32_t n, m;
+    tc_elem(tid, j, n, m);
+    reg[j] = (line0 + n < nlines) ? in[(line0 + n) * kTcR + m] : make_float2(0.0f, 0.0f);
+  }
+}
+
+// Splits the registers of a tile into the buffer's high and low operand halves.
+__device__ inline void tc_split(const float2* reg, unsigned char* bh, unsigned char* bl,
+                                uint32_t inverse, uint32_t tid) {
+#pragma unroll
+  for (uint32_t j = 0; j < kTcPer; ++j) {
+    uint32_t n, m;
+    tc_elem(tid, j, n, m);
+    float2 v = reg[j];
+    if (inverse) v.y = -v.y;
+    const float hr = tf32_hi(v.x), hi = tf32_hi(v.y);
+    *reinterpret_cast<float*>(bh + tc_off(n, m)) = hr;
+    *reinterpret_cast<float*>(bl + tc_off(n, m)) = v.x - hr;
+    *reinterpret_cast<float*>(bh + tc_off(n, kTcR + m)) = hi;
+    *reinterpret_cast<float*>(bl + tc_off(n, kTcR + m)) = v.y - hi;
+  }
+}
+
+// Persistent, software-pipelined: while the MMAs of tile i+1 run and the
+// loads of tile i+2 are in flight, tile i's accumulator is read out and
+// stored.  Two operand buffers (each the staging area of its tile's output
+// once its MMAs are done), two TMEM accumulators, two mbarriers.
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_dft64_tc(const float2* __restrict__ in, float2* __restrict__ out, const float* __restrict__ atab,
                uint64_t nlines, float scale, uint32_t inverse, unsigned int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char* sAh = sm;
   unsigned char* sAl = sm + kTcABytes;
-  unsigned char* sBh = sm + 2 * kTcABytes;
-  unsigned char* sBl = sBh + kTcBBytes;
-  float* stage = reinterpret_cast<float*>(sBh);  // 64 x 129 floats, after the MMAs
-  __shared__ __align__(8) uint64_t mbar;
+  unsigned char* sB = sm + 2 * kTcABytes;  // buffer b: high half at b * 2 kTcBBytes, low half after it
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t s_taddr;
+  __shared__ uint32_t s_fail;
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-  // the split halves of A, once per CTA
   {
     const uint4* src = reinterpret_cast<const uint4*>(atab);
     uint4* dst = reinterpret_cast<uint4*>(sm);
     for (uint32_t i = tid; i < 2 * kTcABytes / 16; i += kTcThreads) dst[i] = src[i];
   }
-  const uint32_t mb = smem_u32(&mbar);
+  const uint32_t mb0 = smem_u32(&mbar[0]), mb1 = smem_u32(&mbar[1]);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_taddr)),
-                 "r"(kTcN)
+                 "r"(2 * kTcN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -146,82 +188,95 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t taddr = s_taddr;
-  uint32_t parity = 0;
-  bool ok = true;
   const uint64_t ntiles = (nlines + kTcN - 1) / kTcN;
-  for (uint64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const uint64_t line0 = tile * kTcN;
-    // lines -> split B halves: line n's complex m gives k = m (re) and 64 + m (im)
-    for (uint32_t e = tid; e < kTcN * kTcR; e += kTcThreads) {
-      const uint32_t n = e >> 6, m = e & 63;
-      float2 v = make_float2(0.0f, 0.0f);
-      if (line0 + n < nlines) v = in[(line0 + n) * kTcR + m];
-      if (inverse) v.y = -v.y;
-      const float hr = tf32_hi(v.x), hi = tf32_hi(v.y);
-      *reinterpret_cast<float*>(sBh + tc_off(n, m)) = hr;
-      *reinterpret_cast<float*>(sBl + tc_off(n, m)) = v.x - hr;
-      *reinterpret_cast<float*>(sBh + tc_off(n, kTcR + m)) = hi;
-      *reinterpret_cast<float*>(sBl + tc_off(n, kTcR + m)) = v.y - hi;
-    }
-    // generic-proxy writes of the operands become visible to the tensor core
+  const uint64_t step = gridDim.x;
+  uint32_t parity[2] = {0, 0};
+  bool pending[2] = {false, false};  // MMAs committed to mbar[b] and not yet waited for
+  auto bufh = [&](uint32_t b) { return sB + b * 2 * kTcBBytes; };
+  auto bufl = [&](uint32_t b) { return sB + b * 2 * kTcBBytes + kTcBBytes; };
+  // split registers into buffer b and issue its MMAs into accumulator b
+  auto launch_tile = [&](const float2* reg, uint32_t b) {
+    tc_split(reg, bufh(b), bufl(b), inverse, tid);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (tid == 0) {
       const uint32_t a[3] = {smem_u32(sAh), smem_u32(sAh), smem_u32(sAl)};
-      const uint32_t b[3] = {smem_u32(sBh), smem_u32(sBl), smem_u32(sBh)};
+      const uint32_t bb[3] = {smem_u32(bufh(b)), smem_u32(bufl(b)), smem_u32(bufh(b))};
+      const uint32_t d = taddr + b * kTcN;
 #pragma unroll 1
       for (int prod = 0; prod < 3; ++prod)
 #pragma unroll 1
         for (uint32_t s = 0; s < kTcK / 8; ++s)
-          tc_mma(taddr, tc_desc(a[prod] + 256 * s), tc_desc(b[prod] + 256 * s),
+          tc_mma(d, tc_desc(a[prod] + 256 * s), tc_desc(bb[prod] + 256 * s),
                  (prod | s) != 0 ? 1u : 0u);
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                       mb)
+                       b ? mb1 : mb0)
                    : "memory");
     }
-    bool done = mbar_wait(mb, parity);
-    if (!done) {
-      // record the failure, then give the MMAs a second bounded wait so that
-      // tensor memory is not freed under them
-      if (tid == 0) atomicOr(err, 1u);
-      done = mbar_wait(mb, parity);
-      ok = false;
+    pending[b] = true;
+  };
+  float2 reg[kTcPer];
+  uint64_t t = blockIdx.x;
+  if (t < ntiles) {
+    tc_load(in, t * kTcN, nlines, tid, reg);
+    launch_tile(reg, 0);
+    if (t + step < ntiles) tc_load(in, (t + step) * kTcN, nlines, tid, reg);
+  }
+  for (uint32_t i = 0; t < ntiles; ++i, t += step) {
+    const uint32_t cur = i & 1, nxt = cur ^ 1;
+    // next tile: its registers were loaded during the previous round
+    if (t + step < ntiles) {
+      launch_tile(reg, nxt);
+      if (t + 2 * step < ntiles) tc_load(in, (t + 2 * step) * kTcN, nlines, tid, reg);
     }
-    parity ^= 1;
+    // this tile's MMAs
+    bool done = mbar_wait(cur ? mb1 : mb0, parity[cur]);
+    if (!done) {
+      if (tid == 0) atomicOr(err, 1u);
+      s_fail = 1;
+      done = mbar_wait(cur ? mb1 : mb0, parity[cur]);  // second bounded wait before moving on
+    }
+    parity[cur] ^= 1;
+    pending[cur] = false;
     tc_fence_after();
-    __syncthreads();  // every thread agrees on ok; the operands are consumed
-    if (!ok) break;
-    // accumulator row r = 32 (warp % 4) + lane: output index r (re, r < 64)
-    // or r - 64 (im); warpgroup warp / 4 reads columns (lines) 32 (warp / 4) ..
-    uint32_t v[kTcN / 2];
-    const uint32_t c0 = (warp >> 2) * (kTcN / 2);
-#pragma unroll
-    for (uint32_t c = 0; c < kTcN / 2; c += 16)
-      tc_ld16(taddr + ((32 * (warp & 3)) << 16) + c0 + c, v + c);
+    __syncthreads();
+    if (s_fail) break;
+    // accumulator row r = 32 (warp % 4) + lane: output r (re, r < 64) or r - 64 (im);
+    // warpgroup warp / 4 reads lines 16 (warp / 4) .. + 16
+    uint32_t v[16];
+    const uint32_t c0 = (warp >> 2) * 16;
+    tc_ld16(taddr + ((32 * (warp & 3)) << 16) + cur * kTcN + c0, v);
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    float* stage = reinterpret_cast<float*>(bufh(cur));  // kTcN x 129 floats
     const uint32_t r = 32 * (warp & 3) + lane;
 #pragma unroll
-    for (uint32_t n = 0; n < kTcN / 2; ++n) stage[(c0 + n) * 129 + r] = __uint_as_float(v[n]);
+    for (uint32_t n = 0; n < 16; ++n) stage[(c0 + n) * 129 + r] = __uint_as_float(v[n]);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    for (uint32_t e = tid; e < kTcN * kTcR; e += kTcThreads) {
-      const uint32_t n = e >> 6, m = e & 63;
+    const uint64_t line0 = t * kTcN;
+#pragma unroll
+    for (uint32_t j = 0; j < kTcPer; ++j) {
+      const uint32_t e = tid + j * kTcThreads, n = e >> 6, m = e & 63;
       if (line0 + n < nlines) {
         float2 y = make_float2(stage[n * 129 + m] * scale, stage[n * 129 + kTcR + m] * scale);
         if (inverse) y.y = -y.y;
         out[(line0 + n) * kTcR + m] = y;
       }
     }
-    __syncthreads();  // the staging area is the next tile's operand area
+    __syncthreads();  // the staging area becomes an operand buffer again
   }
+  // no MMA may still write tensor memory when it is freed
+  for (uint32_t b = 0; b < 2; ++b)
+    if (pending[b]) mbar_wait(b ? mb1 : mb0, parity[b]);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(kTcN)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr),
+                 "r"(2 * kTcN)
                  : "memory");
 }
 

@@ -2,7 +2,7 @@
 profile a kernel in isolation (e.g. under ncu).
 
 python -m wgpufft_b200.profile_case --shape 1024 --batch 32768 [--iters 5]
-       [--precision f32|f64|df64] [--inverse] [--kind c2c|r2c|c2r]
+       [--precision f32|f64|df64] [--inverse] [--kind c2c|r2c|c2r] [--tensor-cores]
 """
 from __future__ import annotations
 
@@ -17,6 +17,8 @@ def main() -> None:
     ap.add_argument("--precision", default="f32", choices=["f32", "f64", "df64"])
     ap.add_argument("--kind", default="c2c", choices=["c2c", "r2c", "c2r"])
     ap.add_argument("--inverse", action="store_true")
+    ap.add_argument("--tensor-cores", action="store_true",
+                    help="tuning tensor_cores = 1 (length-64 f32 lines on the tcgen05 layer)")
     args = ap.parse_args()
     import torch
 
@@ -24,6 +26,8 @@ def main() -> None:
     prec = {"f32": w.FftPrecision.F32, "f64": w.FftPrecision.F64, "df64": w.FftPrecision.Df64}
     cfg = (w.FftConfig.new_nd(args.shape).with_batch(args.batch)
            .with_precision(prec[args.precision]))
+    if args.tensor_cores:
+        cfg = cfg.with_tuning(w.FftTuning().with_tensor_cores(True))
     if args.inverse or args.kind == "c2r":
         cfg = cfg.with_direction(w.FftDirection.Inverse)
     plan = getattr(w.FftPlan, args.kind)(cfg, device=0)
