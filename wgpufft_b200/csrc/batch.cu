@@ -312,14 +312,7 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     }
     d.dM = make_fastdiv((uint32_t)M);
     d.dMN = make_fastdiv((uint32_t)(M - N));
-    li.bhat.assign(M, cd(0, 0));
-    for (uint64_t m = 0; m < N; ++m) {
-      const cd c = std::conj(chirp_fwd(m, N));
-      li.bhat[m] = c;
-      if (m) li.bhat[M - m] = c;
-    }
-    host_fft_fwd(li.bhat);
-    for (auto& x : li.bhat) x /= (double)M;
+    li.bhat = chirp_spectrum(N, M);
   }
   const double T = d.M;
   li.cost = T * std::log2(std::max(2.0, T)) * (d.kind == BK_BLUE || d.kind == BK_CL_BLUE ? 3 : 1);

@@ -6,9 +6,11 @@
 // Roots come from long double sin/cos of the exactly reduced angle, so each
 // table entry is rounded once.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 namespace b2f {
@@ -33,7 +35,38 @@ inline cd chirp_fwd(uint64_t n, uint64_t N) {
 
 // Unnormalised forward DFT of any length: recursive decimation in time that
 // splits off the smallest factor, plain DFT for prime lengths up to 64 and
-// Bluestein over a power of two above.
+// Bluestein over a power of two above.  Large transforms run their top
+// levels on several host threads.
 void host_fft_fwd(std::vector<cd>& x);
+
+// r[k] = exp(-2 pi i k / M) for k < M (r is resized): each root is computed
+// once per octant as root_fwd does and mirrored through the exact
+// symmetries of the unit circle (conjugation, the quarter-turn swap), on
+// several host threads for large M.
+void fill_roots(std::vector<cd>& r, uint64_t M);
+
+// The Bluestein spectrum of a length-N line over a length-M convolution:
+// FFT_M of the conjugate chirp (b[m] = b[M-m] = conj(chirp(m)), zero in the
+// middle), divided by M.
+std::vector<cd> chirp_spectrum(uint64_t N, uint64_t M);
+
+// Runs f(begin, end) over [0, n) split across host threads (one call when n
+// is small).
+template <class F>
+void parallel_ranges(uint64_t n, F f);
+
+template <class F>
+void parallel_ranges(uint64_t n, F f) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const uint64_t nt = n < (1u << 15) ? 1 : std::min<uint64_t>(hw, n >> 14);
+  if (nt <= 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (uint64_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t] { f(n * t / nt, n * (t + 1) / nt); });
+  for (auto& x : th) x.join();
+}
 
 }  // namespace b2f

@@ -423,8 +423,10 @@ struct Builder {
       d.tw_off = (uint32_t)tw.size();
       d.dNs = make_fastdiv((uint32_t)Ns);
       d.dNR = make_fastdiv((uint32_t)(n / R));
+      std::vector<cd> rt;
+      fill_roots(rt, Ns * R);
       for (uint64_t k = 0; k < Ns; ++k)
-        for (uint32_t q = 1; q < R; ++q) tw.push_back(root_fwd(q * k, Ns * R));
+        for (uint32_t q = 1; q < R; ++q) tw.push_back(rt[(q * k) % (Ns * R)]);
       Ns *= R;
     }
     return true;
@@ -682,14 +684,7 @@ static b2f_status add_bluestein_pass(Builder& b, int axis, uint64_t N, const Lin
   Builder::fill_io_grid(lp, ps, outer_n);
   bp.dM = make_fastdiv((uint32_t)M);
   bp.dMN = make_fastdiv((uint32_t)(M - N));
-  std::vector<cd> bvec(M, cd(0, 0));
-  for (uint64_t m = 0; m < N; ++m) {
-    const cd c = std::conj(chirp_fwd(m, N));
-    bvec[m] = c;
-    if (m) bvec[M - m] = c;
-  }
-  host_fft_fwd(bvec);
-  for (auto& x : bvec) x /= (double)M;
+  const std::vector<cd> bvec = chirp_spectrum(N, M);
   b.set_table(b.next_pass(), Builder::F_BLUE_BHAT, b.add_table(b.pack_complex(bvec)));
   b.plan.passes.push_back(ps);
   return B2F_OK;
@@ -750,14 +745,7 @@ static b2f_status add_bluestein_large(Builder& b, int axis, uint64_t N, uint64_t
   mid.label = "bluestein-spectrum-product-stage";
   mid.belem.mode = BE_MID;
   mid.belem.flags = 0;
-  std::vector<cd> bvec(M, cd(0, 0));
-  for (uint64_t m = 0; m < N; ++m) {
-    const cd c = std::conj(chirp_fwd(m, N));
-    bvec[m] = c;
-    if (m) bvec[M - m] = c;
-  }
-  host_fft_fwd(bvec);
-  for (auto& x : bvec) x /= (double)M;
+  const std::vector<cd> bvec = chirp_spectrum(N, M);
   b.set_table(b.next_pass(), Builder::F_BELEM_BHAT, b.add_table(b.pack_complex(bvec)));
   b.plan.passes.push_back(mid);
   st = add_complex_axis(b, axis, AxisKind::Mixed, M, 1, nlines, false, false, 1.0, &cur, BUF_WS2,
