@@ -102,12 +102,10 @@ def test_served_results_match_oracle(cuda):
     rng = np.random.default_rng(2)
     srv = w.FftServer(streams=2)
     cfg = w.FftConfig.new(2048).with_batch(4)
-    ins, outs, ids = [], [], []
-    for _ in range(8):
-        hin, hout = host_arrays(cfg, w.FftTransformKind.C2c, rng)
-        ids.append(srv.submit(cfg, w.FftTransformKind.C2c, hin, hout))
-        ins.append(hin)
-        outs.append(hout)
+    # a burst: the inputs are ready first, then eight identical requests
+    # arrive back to back and are coalesced while their plan is built
+    ins, outs = zip(*[host_arrays(cfg, w.FftTransformKind.C2c, rng) for _ in range(8)])
+    ids = [srv.submit(cfg, w.FftTransformKind.C2c, hin, hout) for hin, hout in zip(ins, outs)]
     srv.drain(60.0)
     for i, hin, hout in zip(ids, ins, outs):
         srv.wait(i, 10.0)

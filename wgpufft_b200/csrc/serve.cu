@@ -17,12 +17,7 @@
 //     stream-ordered free, so copies of one group overlap the kernels of
 //     another;
 //   - resident plans: plans (and their tables/workspaces) are cached by
-//     configuration and reused;
-//   - asynchronous planning: a plan that is not resident yet is built by a
-//     pool of planner threads as soon as its request is submitted, so host
-//     planning runs on several cores and overlaps the GPU work of earlier
-//     groups; the scheduler launches, in queue order, the groups whose plans
-//     are ready and lets the others wait for theirs.
+//     configuration and reused.
 // Completion is observed with events; waiting clients are woken, latency is
 // recorded from submission to completion.
 #include <algorithm>
@@ -30,7 +25,6 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
-#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -87,28 +81,14 @@ struct Server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
-  std::list<SReq*> queue;
+  std::deque<SReq*> queue;
   std::unordered_map<uint64_t, std::unique_ptr<SReq>> reqs;
   std::vector<SGroup> inflight;
   uint64_t used = 0;
   uint64_t next_id = 1;
   int next_stream = 0;
-  // plan cache: key (with the total batch) -> slot, filled by the planners
-  struct PlanSlot {
-    std::unique_ptr<Plan> plan;
-    b2f_status st = B2F_OK;
-    std::string err;
-    bool ready = false;
-  };
-  struct PlanJob {
-    std::string key;
-    Config cfg;
-    int32_t kind;
-  };
-  std::map<std::string, std::unique_ptr<PlanSlot>> plans;
-  std::deque<PlanJob> plan_jobs;
-  std::vector<std::thread> planners;
-  std::condition_variable cv_plan;
+  // plan cache: key (with the total batch) -> plan
+  std::map<std::string, std::unique_ptr<Plan>> plans;
   uint64_t plan_bytes = 0;
   // statistics
   std::vector<double> lat;
@@ -122,10 +102,7 @@ struct Server {
       stop = true;
     }
     cv_work.notify_all();
-    cv_plan.notify_all();
     if (worker.joinable()) worker.join();
-    for (auto& t : planners)
-      if (t.joinable()) t.join();
     cudaSetDevice(device);
     for (auto& g : inflight) {
       cudaEventSynchronize(g.done);
@@ -134,45 +111,16 @@ struct Server {
     for (auto s : streams) cudaStreamDestroy(s);
   }
 
-  // The slot of cfg's plan (lock held); asks the planners for it when it is
-  // not resident and not being built.
-  PlanSlot* request_plan(const Config& cfg, int32_t kind) {
+  Plan* get_plan(const Config& cfg, int32_t kind, b2f_status* st) {
     const std::string k = config_key(cfg, kind) + "|b" + std::to_string(cfg.batch);
     auto it = plans.find(k);
     if (it != plans.end()) return it->second.get();
-    PlanSlot* slot = (plans[k] = std::unique_ptr<PlanSlot>(new PlanSlot())).get();
-    plan_jobs.push_back(PlanJob{k, cfg, kind});
-    cv_plan.notify_one();
-    return slot;
-  }
-
-  // A planner thread: builds plans outside the lock.
-  void plan_loop() {
-    cudaSetDevice(device);
-    std::unique_lock<std::mutex> lk(mu);
-    while (true) {
-      cv_plan.wait(lk, [&] { return stop || !plan_jobs.empty(); });
-      if (plan_jobs.empty()) {
-        if (stop) break;
-        continue;
-      }
-      PlanJob job = std::move(plan_jobs.front());
-      plan_jobs.pop_front();
-      lk.unlock();
-      Plan* p = nullptr;
-      const b2f_status st = create_plan(job.cfg, job.kind, device, &p);
-      const std::string err = st ? last_error() : std::string();
-      lk.lock();
-      PlanSlot* slot = plans[job.key].get();
-      slot->st = st;
-      slot->err = err;
-      if (p) {
-        slot->plan.reset(p);
-        plan_bytes += p->workspace_total() + p->table_bytes;
-      }
-      slot->ready = true;
-      cv_work.notify_all();
-    }
+    Plan* p = nullptr;
+    *st = create_plan(cfg, kind, device, &p);
+    if (*st) return nullptr;
+    plan_bytes += p->workspace_total() + p->table_bytes;
+    plans[k].reset(p);
+    return p;
   }
 
   // Completes every group whose event has fired (lock held).
@@ -208,15 +156,19 @@ struct Server {
     cv_done.notify_all();
   }
 
-  // Launches one group on its (ready) plan (lock held; the CUDA calls are
-  // asynchronous).
-  void launch(std::vector<SReq*>& members, Plan* plan) {
-    uint64_t in_total = 0, out_total = 0;
+  // Launches one group (lock held; the CUDA calls are asynchronous).
+  void launch(std::vector<SReq*>& members) {
+    SReq* r0 = members[0];
+    Config cfg = r0->cfg;
+    uint64_t total_batch = 0, in_total = 0, out_total = 0;
     for (SReq* r : members) {
+      total_batch += r->cfg.batch;
       in_total += r->in_bytes;
       out_total += r->out_bytes;
     }
+    cfg.batch = total_batch;
     b2f_status st = B2F_OK;
+    Plan* plan = get_plan(cfg, r0->kind, &st);
     auto fail_all = [&](b2f_status s, const std::string& msg) {
       for (SReq* r : members) {
         r->state = 3;
@@ -226,6 +178,10 @@ struct Server {
       }
       cv_done.notify_all();
     };
+    if (!plan) {
+      fail_all(st, last_error());
+      return;
+    }
     const int si = next_stream;
     next_stream = (next_stream + 1) % nstreams;
     cudaStream_t s = streams[si];
@@ -276,53 +232,31 @@ struct Server {
                        [&] { return stop || !queue.empty() || !inflight.empty(); });
       if (stop && queue.empty() && inflight.empty()) break;
       reap(false);
-      // admit and group, in queue order: a request, with every later queued
-      // request of the same configuration (continuous batching), runs as
-      // soon as the plan of the group's total batch is ready, or alone on its
-      // own plan; requests whose plans are still being built wait
-      for (auto it = queue.begin(); it != queue.end();) {
-        SReq* head = *it;
-        std::vector<std::list<SReq*>::iterator> pos;
-        uint64_t total_batch = 0, need = 0;
-        for (auto jt = it; jt != queue.end() && pos.size() < max_group; ++jt) {
-          SReq* r = *jt;
-          if (r->key != head->key || (!coalesce && !pos.empty())) continue;
-          const uint64_t b = r->in_bytes + r->out_bytes;
-          if (!pos.empty() && used + need + b > budget) break;
-          pos.push_back(jt);
-          total_batch += r->cfg.batch;
-          need += b;
-        }
-        Config gcfg = head->cfg;
-        gcfg.batch = total_batch;
-        PlanSlot* slot = request_plan(gcfg, head->kind);
-        if (!slot->ready && pos.size() > 1) {
-          // the group's plan is not built yet: run the head alone if its own is
-          PlanSlot* own = request_plan(head->cfg, head->kind);
-          if (own->ready) {
-            slot = own;
-            pos.resize(1);
-            need = head->in_bytes + head->out_bytes;
-          }
-        }
-        if (!slot->ready) {
-          ++it;
-          continue;
-        }
+      // admit and group: take the queue head's configuration, then every
+      // other queued request with the same configuration (continuous batching)
+      while (!queue.empty()) {
+        SReq* head = queue.front();
         std::vector<SReq*> members;
-        for (auto p : pos) members.push_back(*p);
-        if (slot->st != B2F_OK) {
-          for (SReq* r : members) {
-            r->state = 3;
-            r->status = slot->st;
-            r->error = slot->err;
-            ++failed;
+        uint64_t need = 0;
+        for (auto it = queue.begin(); it != queue.end() && members.size() < max_group;) {
+          SReq* r = *it;
+          if (r->key != head->key || (!coalesce && !members.empty())) {
+            ++it;
+            continue;
           }
-          cv_done.notify_all();
-        } else if (used + need > budget && !inflight.empty()) {
-          reap(true);  // wait for memory, then look at the queue again
+          const uint64_t b = r->in_bytes + r->out_bytes;
+          if (!members.empty() && used + need + b > budget) break;
+          members.push_back(r);
+          need += b;
+          it = queue.erase(it);
+        }
+        if (used + need > budget && !inflight.empty()) {
+          // wait for memory: put them back in front, in order
+          for (auto it = members.rbegin(); it != members.rend(); ++it) queue.push_front(*it);
+          reap(true);
           break;
-        } else if (used + need > budget) {
+        }
+        if (used + need > budget) {
           for (SReq* r : members) {
             r->state = 3;
             r->status = B2F_ERR_RESOURCE_ALLOCATION;
@@ -330,13 +264,9 @@ struct Server {
             ++failed;
           }
           cv_done.notify_all();
-        } else {
-          launch(members, slot->plan.get());
+          continue;
         }
-        // drop the group from the queue and look at it again from the front
-        // (earlier requests may have had their plans finished meanwhile)
-        for (auto p : pos) queue.erase(p);
-        it = queue.begin();
+        launch(members);
         // bound the work in flight: at most two groups per stream
         if ((int)inflight.size() >= 2 * nstreams) reap(true);
       }
@@ -373,8 +303,6 @@ b2f_status b2f_server_new(b2f_server** out, int32_t device, uint64_t hbm_budget_
     s->streams.push_back(st);
   }
   Server* raw = s.get();
-  const unsigned np = std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
-  for (unsigned i = 0; i < np; ++i) s->planners.emplace_back([raw] { raw->plan_loop(); });
   s->worker = std::thread([raw] { raw->run(); });
   *out = new b2f_server{s.release()};
   return B2F_OK;
@@ -427,7 +355,6 @@ b2f_status b2f_server_submit(b2f_server* srv, const b2f_config* cfg, int32_t kin
     if (s->t_first == 0) s->t_first = r->t_submit;
     *request_id = r->id;
     s->queue.push_back(r.get());
-    s->request_plan(r->cfg, kind);  // start building its plan now
     s->reqs[r->id] = std::move(r);
   }
   s->cv_work.notify_one();
