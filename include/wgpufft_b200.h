@@ -185,9 +185,9 @@ void b2f_recorder_free(b2f_recorder* rec);
  * line i has lengths[i] points at complex offset offsets[i] of the input and
  * output buffers (lines must not overlap); direction and normalization are
  * shared.  Lines that fit one CTA are taken from a device work queue by
- * persistent CTAs; longer lines (up to ~100k points, Bluestein lengths up
- * to ~50k) run on 8-CTA thread-block clusters through distributed shared
- * memory, one HBM pass each. */
+ * persistent CTAs; longer lines run as a column pass and a row pass (three
+ * passes for Bluestein lengths) through a scratch region, their column and
+ * row groups taken from a second work queue. */
 typedef struct b2f_batch b2f_batch;
 b2f_status b2f_batch_new(b2f_batch** out, const uint64_t* lengths, const uint64_t* offsets,
                          uint64_t count, int32_t direction, int32_t normalization,
@@ -213,6 +213,19 @@ b2f_status b2f_batch_execute(const b2f_batch* batch, void* stream, const void* i
 b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const void* in,
                                    uint64_t in_bytes, void* out, uint64_t out_bytes,
                                    uint32_t parts, int32_t sequential);
+/* b2f_batch_execute from and to host memory: the lines are cut, in offset
+ * order, into 8 chunks of about equal bytes, and chunk c's copy in
+ * (host_in -> dev_in), transform (dev_in -> dev_out) and copy out
+ * (dev_out -> host_out) overlap the other chunks' on three internal
+ * streams; `stream` orders the whole call with the caller's work (the call
+ * is asynchronous: the results are in host_out once `stream` has reached
+ * this point).  Each of the four buffers holds `bytes` >=
+ * b2f_batch_required_buffer_size_bytes; host_in == host_out and dev_in ==
+ * dev_out are allowed.  Host buffers should be page-locked for the copies
+ * to overlap.  Batches with cluster lines (B2F_BATCH_CLUSTERS) run
+ * unchunked: copy in, execute, copy out. */
+b2f_status b2f_batch_execute_host(const b2f_batch* batch, void* stream, const void* host_in,
+                                  void* host_out, void* dev_in, void* dev_out, uint64_t bytes);
 /* Task and launch summary as JSON (same length convention as the plan's). */
 b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_t* len);
 

@@ -29,6 +29,21 @@ def test_library_exports_every_declared_symbol():
     assert L.b2f_version().startswith(b"wgpufft_b200")
 
 
+def test_python_binding_declares_every_symbol_with_its_arity():
+    # a symbol without argtypes would pass 64-bit pointers as C ints
+    src = open(os.path.join(ROOT, "include", "wgpufft_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    L = w.lib()
+    protos = re.findall(r"\b(b2f_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src)
+    assert len(protos) >= 30
+    for name, params in protos:
+        params = params.strip()
+        arity = 0 if params in ("", "void") else params.count(",") + 1
+        fn = getattr(L, name)
+        assert fn.argtypes is not None, name
+        assert len(fn.argtypes) == arity, name
+
+
 def test_status_strings_name_reference_variants():
     L = w.lib()
     assert L.b2f_status_string(1) == b"ZeroLength"

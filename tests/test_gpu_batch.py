@@ -108,3 +108,46 @@ def test_batch_rejects_overlap_and_small_buffers(cuda):
     with pytest.raises(w.FftError) as e:
         b.execute(t, t)
     assert e.value.kind == "BufferViewTooSmall"
+
+
+def _host_run(b, x, in_place=False):
+    import torch
+    hin = torch.from_numpy(x.view(np.float32).copy()).pin_memory()
+    hout = hin if in_place else torch.empty_like(hin).pin_memory()
+    din = torch.empty(hin.numel(), dtype=torch.float32, device="cuda")
+    dout = din if in_place else torch.empty_like(din)
+    b.execute_host(hin, hout, din, dout)
+    torch.cuda.synchronize()
+    return hout.numpy().view(np.complex64).copy()
+
+
+@pytest.mark.parametrize("lengths", [
+    W.mixed_lengths(),                      # the 20,000-line workload: 8 chunks
+    np.array(SMALL),                        # every route, chunks of a few lines
+    np.array([4099, 65536, 17]),            # fewer lines than chunks
+])
+def test_batch_execute_host_matches_device_execute(cuda, lengths):
+    # chunked copy-in / transform / copy-out: the same bits as the
+    # device-resident execution, in place too
+    x, y, off, b = run_batch(lengths, seed=11)
+    assert np.array_equal(_host_run(b, x), y)
+    assert np.array_equal(_host_run(b, x, in_place=True), y)
+
+
+def test_batch_execute_host_gaps_inverse_and_clusters(cuda):
+    import torch
+    lengths = np.array([1024, 30011, 4096, 65536, 100])
+    off = np.array([5, 2000, 40000, 50000, 130000])  # unpacked, out of order lines
+    off = off[[2, 0, 4, 1, 3]]
+    lengths = lengths[[2, 0, 4, 1, 3]]
+    total = int((off + lengths).max())
+    x = W.normal_complex(total, 12)
+    for clusters in (False, True):
+        b = w.FftBatch(lengths, off, w.FftDirection.Inverse, clusters=clusters)
+        y = _host_run(b, x)
+        check_lines(x, y, lengths, off, range(len(lengths)), inverse=True)
+    hb = torch.empty(8, dtype=torch.float32)
+    db = torch.empty(8, dtype=torch.float32, device="cuda")
+    with pytest.raises(w.FftError) as e:
+        b.execute_host(hb, hb, db, db)
+    assert e.value.kind == "BufferViewTooSmall"

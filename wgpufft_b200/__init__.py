@@ -107,6 +107,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_batch_execute": (st, [vp, vp, vp, u64, vp, u64]),
         "b2f_batch_diagnostics_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
         "b2f_batch_execute_parts": (st, [vp, vp, vp, u64, vp, u64, u32, i32]),
+        "b2f_batch_execute_host": (st, [vp, vp, vp, vp, vp, vp, u64]),
+        "b2f_c2c_1d_f32_noalloc": (st, [vp, vp, u64, vp, u64, u64, u64, i32, i32]),
         "b2f_server_new": (st, [pvp, i32, u64, i32, i32]),
         "b2f_server_free": (None, [vp]),
         "b2f_server_submit": (st, [vp, vp, i32, vp, u64, vp, u64, ctypes.POINTER(u64)]),
@@ -568,6 +570,27 @@ class FftBatch:
         _check(lib().b2f_batch_execute_parts(self._ptr, _stream(stream), ip, ib, op, ob, parts,
                                              int(sequential)))
 
+    def execute_host(self, host_in, host_out, dev_in, dev_out, stream=None) -> None:
+        """From and to host memory (b2f_batch_execute_host): the chunks'
+        copies in, transforms and copies out overlap.  host_in/host_out are
+        CPU tensors (page-locked for the copies to overlap) or (address,
+        nbytes) pairs; dev_in/dev_out are the device staging buffers.
+        Asynchronous on `stream` like execute()."""
+        def host(b):
+            if isinstance(b, tuple):
+                return int(b[0]), int(b[1])
+            if hasattr(b, "data_ptr"):
+                if b.is_cuda:
+                    raise FftError("InvalidArgument", 15, "host buffers must be CPU memory")
+                return int(b.data_ptr()), int(b.numel() * b.element_size())
+            raise TypeError("buffer must be a torch CPU tensor or an (address, nbytes) pair")
+        hi, hib = host(host_in)
+        ho, hob = host(host_out)
+        di, dib = _buf(dev_in)
+        do, dob = _buf(dev_out)
+        _check(lib().b2f_batch_execute_host(self._ptr, _stream(stream), hi, ho, di, do,
+                                            min(hib, hob, dib, dob)))
+
     def diagnostics(self) -> dict:
         L = lib()
         n = ctypes.c_uint64(0)
@@ -643,12 +666,18 @@ class FftServer:
 
 
 # ---------------------------------------------------- autotuner and snapshot
-def _json_out(fn, *args) -> str:
-    n = ctypes.c_uint64(0)
-    _check(fn(*args, None, ctypes.byref(n)))
-    buf = ctypes.create_string_buffer(n.value + 1)
-    n2 = ctypes.c_uint64(n.value + 1)
-    _check(fn(*args, buf, ctypes.byref(n2)))
+def _json_out(fn, *args, cap: int = 1 << 20) -> str:
+    """One call into a buffer of `cap` bytes (the autotuner runs once per
+    call, so its report is not sized by a first call); a second, larger call
+    only when the text did not fit."""
+    buf = ctypes.create_string_buffer(cap)
+    n = ctypes.c_uint64(cap)
+    st = fn(*args, buf, ctypes.byref(n))
+    if st == 12 and n.value >= cap:
+        buf = ctypes.create_string_buffer(n.value + 1)
+        n = ctypes.c_uint64(n.value + 1)
+        st = fn(*args, buf, ctypes.byref(n))
+    _check(st)
     return buf.value.decode()
 
 

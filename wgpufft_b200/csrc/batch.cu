@@ -81,6 +81,15 @@ static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
   return r;
 }
 
+// Host-buffer execution (b2f_batch_execute_host) pipelines the lines in
+// kHostChunks chunks: contiguous runs of lines (in offset order) of about
+// equal bytes, each copied in, transformed and copied out on its own.
+constexpr uint32_t kHostChunks = 8;
+// work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
+// cluster queues, [4 + ph] long-line phase ph; per chunk c of a host
+// execution, [8 + 4c] its CTA tasks and [9 + 4c + ph] its long phase ph
+constexpr unsigned kBatchCounters = 8 + 4 * kHostChunks;
+
 struct BatchPlan {
   int device = 0;
   int32_t direction = B2F_FORWARD, normalization = B2F_NORM_INVERSE;
@@ -88,6 +97,7 @@ struct BatchPlan {
   // device state
   BatchLen* d_lens = nullptr;
   BatchTask* d_tasks = nullptr;  // CTA tasks then cluster tasks
+  BatchTask* d_tasks_chunked = nullptr;  // CTA tasks chunk by chunk
   uint64_t* d_off = nullptr;
   unsigned int* d_counters = nullptr;  // [0] CTA queue, [1] cluster queue
   std::vector<void*> tables;
@@ -97,7 +107,17 @@ struct BatchPlan {
   LongLenDesc* d_long_lens = nullptr;
   LongLine* d_long_lines = nullptr;
   LongTask* d_long_tasks = nullptr;
+  LongTask* d_long_tasks_chunked = nullptr;
   uint32_t long_first[3] = {0, 0, 0}, long_count[3] = {0, 0, 0};
+  // chunks of host execution: element ranges [chunk_lo, chunk_hi) of the
+  // buffers, and each chunk's tasks (CTA queue; long phases, relative to
+  // long_first) -- every task list is ordered by chunk
+  uint64_t chunk_lo[kHostChunks] = {}, chunk_hi[kHostChunks] = {};
+  uint32_t cta_cfirst[kHostChunks] = {}, cta_ccount[kHostChunks] = {};
+  uint32_t long_cfirst[3][kHostChunks] = {}, long_ccount[3][kHostChunks] = {};
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};  // copy in, transform, copy out
+  cudaEvent_t hev_start = nullptr, hev_done = nullptr;
+  cudaEvent_t hev_in[kHostChunks] = {}, hev_c[kHostChunks] = {};
   uint32_t long_cap = 0;
   size_t smem_long = 0;
   unsigned grid_long = 0;
@@ -124,6 +144,7 @@ struct BatchPlan {
     for (void* p : tables) cudaFree(p);
     cudaFree(d_lens);
     cudaFree(d_tasks);
+    cudaFree(d_tasks_chunked);
     cudaFree(d_off);
     cudaFree(d_counters);
     cudaFree(d_scratch);
@@ -131,7 +152,16 @@ struct BatchPlan {
     cudaFree(d_long_lens);
     cudaFree(d_long_lines);
     cudaFree(d_long_tasks);
+    cudaFree(d_long_tasks_chunked);
     if (side) cudaStreamDestroy(side);
+    for (auto h : hs)
+      if (h) cudaStreamDestroy(h);
+    for (uint32_t c = 0; c < kHostChunks; ++c) {
+      if (hev_in[c]) cudaEventDestroy(hev_in[c]);
+      if (hev_c[c]) cudaEventDestroy(hev_c[c]);
+    }
+    if (hev_start) cudaEventDestroy(hev_start);
+    if (hev_done) cudaEventDestroy(hev_done);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
     if (prev >= 0) cudaSetDevice(prev);
@@ -141,9 +171,6 @@ struct BatchPlan {
 constexpr int kClusterP = 8;
 constexpr int kClusterBig = 16;  // non-portable cluster size for the longest Bluestein lines
 constexpr unsigned kCtaThreads = 256;
-// work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
-// cluster queues, [4 + ph] long-line phase ph
-constexpr unsigned kBatchCounters = 8;
 constexpr unsigned kClusterThreads = 512;
 
 struct LenInfo {
@@ -475,7 +502,26 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       li.d.perm_out = (const uint32_t*)b;
     }
   }
-  // tasks: CTA tasks (groups of G lines of one length), cluster tasks (one line each)
+  // chunks of host execution: lines in offset order, cut into runs of about
+  // equal bytes
+  std::vector<uint32_t> chunk_of(nlines, 0);
+  {
+    uint64_t total = 0, acc = 0;
+    for (uint64_t i = 0; i < nlines; ++i) total += lengths[i];
+    for (uint32_t c = 0; c < kHostChunks; ++c) bp->chunk_lo[c] = bp->chunk_hi[c] = 0;
+    bool seen[kHostChunks] = {};
+    for (uint64_t i = 0; i < nlines; ++i) {
+      const uint64_t l = order[i];
+      const uint32_t c = (uint32_t)std::min<uint64_t>(kHostChunks - 1, acc * kHostChunks / total);
+      chunk_of[l] = c;
+      if (!seen[c]) bp->chunk_lo[c] = offsets[l];
+      seen[c] = true;
+      bp->chunk_hi[c] = offsets[l] + lengths[l];
+      acc += lengths[l];
+    }
+  }
+  // tasks: CTA tasks (groups of G lines of one length and one chunk),
+  // cluster tasks (one line each)
   std::vector<uint64_t> sorted_off;
   std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks;
   std::vector<double> cta_cost, cl_cost, big_cost;
@@ -484,6 +530,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   // phases (1: columns, 2: rows, 3: Bluestein inverse columns).
   std::vector<LongLine> long_lines;
   std::vector<LongTask> long_tasks[3];
+  std::vector<uint32_t> long_task_chunk[3];
   uint64_t scratch_total = 0;
   for (size_t li = 0; li < lens_list.size(); ++li) {
     const auto& lines = by_len[lens_list[li]];
@@ -499,20 +546,37 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
         scratch_total += g.M;
         bp->elems_long += lens_list[li];
         bp->lines_long += 1;
-        for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) long_tasks[0].push_back(LongTask{idx, g0});
-        for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr) long_tasks[1].push_back(LongTask{idx, g0});
+        const uint32_t ch = chunk_of[line];
+        for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
+          long_tasks[0].push_back(LongTask{idx, g0});
+          long_task_chunk[0].push_back(ch);
+        }
+        for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr) {
+          long_tasks[1].push_back(LongTask{idx, g0});
+          long_task_chunk[1].push_back(ch);
+        }
         if (g.blue)
-          for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) long_tasks[2].push_back(LongTask{idx, g0});
+          for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
+            long_tasks[2].push_back(LongTask{idx, g0});
+            long_task_chunk[2].push_back(ch);
+          }
       }
       continue;
     }
-    for (size_t s = 0; s < lines.size(); s += (cl ? 1 : d.G)) {
+    std::vector<uint64_t> ls = lines;  // grouped by chunk: a task's lines share one
+    std::stable_sort(ls.begin(), ls.end(),
+                     [&](uint64_t a, uint64_t b) { return chunk_of[a] < chunk_of[b]; });
+    for (size_t s = 0; s < ls.size();) {
+      const uint32_t ch = chunk_of[ls[s]];
+      size_t e = s;
+      while (e < ls.size() && chunk_of[ls[e]] == ch && e - s < (cl ? 1u : d.G)) ++e;
       BatchTask t;
       t.len = (uint32_t)li;
       t.first = (uint32_t)sorted_off.size();
-      t.count = (uint32_t)std::min<size_t>(cl ? 1 : d.G, lines.size() - s);
-      t.pad = 0;
-      for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[lines[s + c]]);
+      t.count = (uint32_t)(e - s);
+      t.pad = ch;  // chunk (not read by the kernels)
+      for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[ls[s + c]]);
+      s = e;
       if (cl && d.P == kClusterBig) {
         big_tasks.push_back(t);
         big_cost.push_back(infos[li].cost);
@@ -541,6 +605,32 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     t.swap(out);
   };
   sort_by_cost(cta_tasks, cta_cost);
+  // the same tasks chunk by chunk (longest first within each), for host
+  // execution; the whole-batch queue keeps the global longest-first order
+  std::vector<BatchTask> cta_chunked = cta_tasks;
+  std::stable_sort(cta_chunked.begin(), cta_chunked.end(),
+                   [](const BatchTask& a, const BatchTask& b) { return a.pad < b.pad; });
+  for (size_t i = 0; i < cta_chunked.size(); ++i) {
+    const uint32_t c = cta_chunked[i].pad;
+    if (bp->cta_ccount[c] == 0) bp->cta_cfirst[c] = (uint32_t)i;
+    ++bp->cta_ccount[c];
+  }
+  // long tasks of each phase chunk by chunk, likewise
+  std::vector<LongTask> long_chunked[3];
+  for (int ph = 0; ph < 3; ++ph) {
+    std::vector<size_t> idx(long_tasks[ph].size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+      return long_task_chunk[ph][a] < long_task_chunk[ph][b];
+    });
+    long_chunked[ph].resize(idx.size());
+    for (size_t i = 0; i < idx.size(); ++i) {
+      long_chunked[ph][i] = long_tasks[ph][idx[i]];
+      const uint32_t c = long_task_chunk[ph][idx[i]];
+      if (bp->long_ccount[ph][c] == 0) bp->long_cfirst[ph][c] = (uint32_t)i;
+      ++bp->long_ccount[ph][c];
+    }
+  }
   sort_by_cost(cl_tasks, cl_cost);
   sort_by_cost(big_tasks, big_cost);
   bp->n_cta = (uint32_t)cta_tasks.size();
@@ -572,8 +662,13 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   bool okc = cudaMalloc(&bp->d_lens, dl.size() * sizeof(BatchLen)) == cudaSuccess &&
              cudaMalloc(&bp->d_tasks, std::max<size_t>(1, all.size()) * sizeof(BatchTask)) == cudaSuccess &&
              cudaMalloc(&bp->d_off, sorted_off.size() * 8) == cudaSuccess &&
-             cudaMalloc(&bp->d_counters, kBatchCounters * sizeof(unsigned int)) == cudaSuccess;
+             cudaMalloc(&bp->d_counters, kBatchCounters * sizeof(unsigned int)) == cudaSuccess &&
+             cudaMalloc(&bp->d_tasks_chunked, std::max<size_t>(1, cta_chunked.size()) * sizeof(BatchTask)) ==
+                 cudaSuccess;
   if (!okc) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch allocation failed");
+  if (!cta_chunked.empty())
+    cudaMemcpy(bp->d_tasks_chunked, cta_chunked.data(), cta_chunked.size() * sizeof(BatchTask),
+               cudaMemcpyHostToDevice);
   cudaMemcpy(bp->d_lens, dl.data(), dl.size() * sizeof(BatchLen), cudaMemcpyHostToDevice);
   if (!all.empty()) cudaMemcpy(bp->d_tasks, all.data(), all.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
   cudaMemcpy(bp->d_off, sorted_off.data(), sorted_off.size() * 8, cudaMemcpyHostToDevice);
@@ -583,16 +678,18 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     std::memset(gl.data(), 0, gl.size() * sizeof(LongLenDesc));
     for (size_t i = 0; i < infos.size(); ++i)
       if (infos[i].d.kind == BK_LONG || infos[i].d.kind == BK_LONG_BLUE) gl[i] = infos[i].lng;
-    std::vector<LongTask> lt;
+    std::vector<LongTask> lt, ltc;
     for (int ph = 0; ph < 3; ++ph) {
       bp->long_first[ph] = (uint32_t)lt.size();
       bp->long_count[ph] = (uint32_t)long_tasks[ph].size();
       lt.insert(lt.end(), long_tasks[ph].begin(), long_tasks[ph].end());
+      ltc.insert(ltc.end(), long_chunked[ph].begin(), long_chunked[ph].end());
     }
     const bool okl =
         cudaMalloc(&bp->d_long_lens, gl.size() * sizeof(LongLenDesc)) == cudaSuccess &&
         cudaMalloc(&bp->d_long_lines, long_lines.size() * sizeof(LongLine)) == cudaSuccess &&
         cudaMalloc(&bp->d_long_tasks, lt.size() * sizeof(LongTask)) == cudaSuccess &&
+        cudaMalloc(&bp->d_long_tasks_chunked, ltc.size() * sizeof(LongTask)) == cudaSuccess &&
         cudaMalloc(&bp->d_scratch, scratch_total * 8) == cudaSuccess;
     if (!okl) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch long-line allocation failed");
     bp->scratch_bytes = scratch_total * 8;
@@ -600,6 +697,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     cudaMemcpy(bp->d_long_lines, long_lines.data(), long_lines.size() * sizeof(LongLine),
                cudaMemcpyHostToDevice);
     cudaMemcpy(bp->d_long_tasks, lt.data(), lt.size() * sizeof(LongTask), cudaMemcpyHostToDevice);
+    cudaMemcpy(bp->d_long_tasks_chunked, ltc.data(), ltc.size() * sizeof(LongTask), cudaMemcpyHostToDevice);
   }
   // launch shapes
   int nsm = 148;
@@ -674,6 +772,16 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       cudaEventCreateWithFlags(&bp->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&bp->join, cudaEventDisableTiming) != cudaSuccess)
     return fail(B2F_ERR_DEVICE, "batch stream creation failed");
+  {
+    bool okh = cudaEventCreateWithFlags(&bp->hev_start, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&bp->hev_done, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 3 && okh; ++i)
+      okh = cudaStreamCreateWithFlags(&bp->hs[i], cudaStreamNonBlocking) == cudaSuccess;
+    for (uint32_t c = 0; c < kHostChunks && okh; ++c)
+      okh = cudaEventCreateWithFlags(&bp->hev_in[c], cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&bp->hev_c[c], cudaEventDisableTiming) == cudaSuccess;
+    if (!okh) return fail(B2F_ERR_DEVICE, "batch host-pipeline stream creation failed");
+  }
   std::ostringstream os;
   os << "{\"lines\":" << nlines << ",\"distinct_lengths\":" << bp->distinct
      << ",\"cta_lines\":" << bp->lines_cta << ",\"cluster_lines\":" << bp->lines_cl
@@ -701,6 +809,9 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   *out = bp.release();
   return B2F_OK;
 }
+
+static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, void* out, int chunk,
+                        cudaError_t* err);
 
 static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in, void* out,
                             uint32_t parts = 7, bool sequential = false) {
@@ -760,24 +871,7 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && (parts & 4) && bp.lines_long) {
-    LongParams lp{};
-    lp.in = (const c32*)in;
-    lp.out = (c32*)out;
-    lp.scratch = bp.d_scratch;
-    lp.tw = bp.d_tw;
-    lp.lens = bp.d_long_lens;
-    lp.lines = bp.d_long_lines;
-    lp.inverse = p.inverse;
-    lp.cap = bp.long_cap;
-    for (uint32_t ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
-      if (bp.long_count[ph] == 0) continue;
-      lp.tasks = bp.d_long_tasks + bp.long_first[ph];
-      lp.ntasks = bp.long_count[ph];
-      lp.phase = ph + 1;
-      lp.counter = bp.d_counters + 4 + ph;
-      k_long_pass<<<bp.grid_long, kLongThreads, bp.smem_long, st>>>(lp);
-      e = cudaGetLastError();
-    }
+    launch_long(bp, st, in, out, -1, &e);
   }
   if (e == cudaSuccess && run_cl && !sequential) {
     e = cudaEventRecord(bp.join, bp.side);
@@ -786,6 +880,109 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
   if (prev >= 0 && prev != bp.device) cudaSetDevice(prev);
   if (e != cudaSuccess) return fail(B2F_ERR_DEVICE, std::string("batch launch failed: ") + cudaGetErrorString(e));
   return B2F_OK;
+}
+
+// The long-line phases of every line (chunk < 0) or of one chunk.
+static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, void* out, int chunk,
+                        cudaError_t* err) {
+  cudaError_t e = cudaSuccess;
+  {
+    LongParams lp{};
+    lp.in = (const c32*)in;
+    lp.out = (c32*)out;
+    lp.scratch = bp.d_scratch;
+    lp.tw = bp.d_tw;
+    lp.lens = bp.d_long_lens;
+    lp.lines = bp.d_long_lines;
+    lp.cap = bp.long_cap;
+    lp.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
+    for (uint32_t ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
+      const uint32_t first = chunk < 0 ? 0 : bp.long_cfirst[ph][chunk];
+      const uint32_t count = chunk < 0 ? bp.long_count[ph] : bp.long_ccount[ph][chunk];
+      if (count == 0) continue;
+      lp.tasks = (chunk < 0 ? bp.d_long_tasks : bp.d_long_tasks_chunked) + bp.long_first[ph] + first;
+      lp.ntasks = count;
+      lp.phase = ph + 1;
+      lp.counter = bp.d_counters + (chunk < 0 ? 4 + ph : 9 + 4 * chunk + ph);
+      const unsigned grid = (unsigned)std::min<uint64_t>(bp.grid_long, (count + kLongChunk - 1) / kLongChunk);
+      k_long_pass<<<grid, kLongThreads, bp.smem_long, st>>>(lp);
+      e = cudaGetLastError();
+    }
+  }
+  *err = e;
+}
+
+// One chunk of a host execution: its CTA tasks and long phases on st (the
+// chunk's counters were zeroed by the caller).
+static cudaError_t run_chunk(const BatchPlan& bp, cudaStream_t st, const void* in, void* out,
+                             int chunk) {
+  cudaError_t e = cudaSuccess;
+  if (bp.cta_ccount[chunk]) {
+    BatchParams pt{};
+    pt.in = (const c32*)in;
+    pt.out = (c32*)out;
+    pt.lens = bp.d_lens;
+    pt.line_off = bp.d_off;
+    pt.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
+    pt.tw = bp.d_tw;
+    pt.tasks = bp.d_tasks_chunked + bp.cta_cfirst[chunk];
+    pt.ntasks = bp.cta_ccount[chunk];
+    pt.counter = bp.d_counters + 8 + 4 * chunk;
+    const unsigned grid = (unsigned)std::min<uint64_t>(bp.grid_cta, bp.cta_ccount[chunk]);
+    k_batch_cta<<<grid, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && bp.lines_long) launch_long(bp, st, in, out, chunk, &e);
+  return e;
+}
+
+// Host buffers in and out: the chunks' copies in (stream hs[0]), transforms
+// (hs[1]) and copies out (hs[2]) overlap, chunk c's transform waiting for
+// its copy in and its copy out for its transform; `st` orders the whole
+// call with the caller's other work.  Cluster routes run unchunked.
+static b2f_status run_batch_host(const BatchPlan& bp, cudaStream_t st, const void* host_in,
+                                 void* host_out, void* dev_in, void* dev_out) {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != bp.device) cudaSetDevice(bp.device);
+  const uint64_t bytes = bp.extent * 8;
+  cudaError_t e = cudaSuccess;
+  auto finish = [&]() -> b2f_status {
+    if (prev >= 0 && prev != bp.device) cudaSetDevice(prev);
+    if (e != cudaSuccess)
+      return fail(B2F_ERR_DEVICE, std::string("batch host execution failed: ") + cudaGetErrorString(e));
+    return B2F_OK;
+  };
+  if (bp.n_cl || bp.n_big) {
+    e = cudaMemcpyAsync(dev_in, host_in, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && run_batch(bp, st, dev_in, dev_out) != B2F_OK) e = cudaErrorLaunchFailure;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, dev_out, bytes, cudaMemcpyDeviceToHost, st);
+    return finish();
+  }
+  cudaStream_t sin = bp.hs[0], sc = bp.hs[1], sout = bp.hs[2];
+  e = cudaEventRecord(bp.hev_start, st);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(bp.hs[i], bp.hev_start, 0);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(bp.d_counters, 0, kBatchCounters * sizeof(unsigned int), sc);
+  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+    const uint64_t lo = bp.chunk_lo[c] * 8, n = (bp.chunk_hi[c] - bp.chunk_lo[c]) * 8;
+    if (n) e = cudaMemcpyAsync((char*)dev_in + lo, (const char*)host_in + lo, n, cudaMemcpyHostToDevice, sin);
+    if (e == cudaSuccess) e = cudaEventRecord(bp.hev_in[c], sin);
+  }
+  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+    e = cudaStreamWaitEvent(sc, bp.hev_in[c], 0);
+    if (e == cudaSuccess) e = run_chunk(bp, sc, dev_in, dev_out, (int)c);
+    if (e == cudaSuccess) e = cudaEventRecord(bp.hev_c[c], sc);
+  }
+  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+    const uint64_t lo = bp.chunk_lo[c] * 8, n = (bp.chunk_hi[c] - bp.chunk_lo[c]) * 8;
+    e = cudaStreamWaitEvent(sout, bp.hev_c[c], 0);
+    if (e == cudaSuccess && n)
+      e = cudaMemcpyAsync((char*)host_out + lo, (const char*)dev_out + lo, n, cudaMemcpyDeviceToHost, sout);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(bp.hev_done, sout);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bp.hev_done, 0);
+  return finish();
 }
 
 }  // namespace b2f
@@ -843,6 +1040,16 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* b, void* stream, const void*
   if (in_bytes < need || out_bytes < need)
     return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall { required: " + std::to_string(need) + " }");
   return run_batch(*b->plan, (cudaStream_t)stream, in, out, parts, sequential != 0);
+}
+
+b2f_status b2f_batch_execute_host(const b2f_batch* b, void* stream, const void* host_in,
+                                  void* host_out, void* dev_in, void* dev_out, uint64_t bytes) {
+  if (!b || !host_in || !host_out || !dev_in || !dev_out)
+    return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
+  const uint64_t need = b->plan->extent * 8;
+  if (bytes < need)
+    return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall { required: " + std::to_string(need) + " }");
+  return run_batch_host(*b->plan, (cudaStream_t)stream, host_in, host_out, dev_in, dev_out);
 }
 
 b2f_status b2f_batch_diagnostics_json(const b2f_batch* b, char* buf, uint64_t* len) {
