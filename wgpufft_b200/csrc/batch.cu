@@ -189,21 +189,69 @@ struct LenInfo {
 // CTAs fit one SM).
 static uint32_t long_lines_log2(uint64_t nx) { return nx <= 208 ? 4 : (nx <= 393 ? 3 : 2); }
 
-// T = N1 * N2 with both factors in [2, 512]: the split whose passes take
-// the most lines per task, then the most balanced; 0 when none exists.
-static uint64_t long_split(uint64_t T) {
+// Estimated cost of one task of a long-line pass of length nx (2..512,
+// 13-smooth): for each stage of radix R, the butterfly rounds the task's 256
+// threads take (ceil(NR / S) rounds of S threads per line, idle threads
+// included) times R points each, weighted by an instruction estimate per
+// point (about 10 for the shared-memory traffic, addressing and twiddle
+// product, plus the radix-R codelet's arithmetic).  0 for other lengths.
+static const std::vector<double>& long_task_costs() {
+  static const std::vector<double> tab = [] {
+    std::vector<double> t(513, 0.0);
+    for (uint32_t nx = 2; nx <= 512; ++nx) {
+      const std::vector<uint32_t> rad = stage_radices(nx);
+      if (rad.empty()) continue;
+      const uint32_t S = kLongThreads >> long_lines_log2(nx);
+      double c = 0;
+      for (uint32_t R : rad) {
+        double f = 0;
+        switch (R) {
+          case 2: f = 2.0; break;
+          case 3: case 4: f = 4.0; break;
+          case 5: f = 6.4; break;
+          case 7: f = 10.3; break;
+          case 8: f = 6.5; break;
+          case 9: f = 8.9; break;
+          case 11: f = 12.7; break;
+          case 13: f = 13.8; break;
+          default: f = 9.0; break;  // 16
+        }
+        const uint32_t rounds = (nx / R + S - 1) / S;
+        c += (double)rounds * R * kLongThreads * (10.0 + f);
+      }
+      t[nx] = c;
+    }
+    return t;
+  }();
+  return tab;
+}
+
+// Estimated cost of a long line over T = a * (T / a): `ffts` transforms
+// through both passes (1 for a smooth line; 2 for Bluestein, forward and
+// inverse) and `passes` HBM passes of about 30 instructions per point.
+static double long_cost(uint64_t T, uint64_t a, int ffts, int passes) {
+  const std::vector<double>& t = long_task_costs();
+  const uint64_t b = T / a;
+  const uint64_t Ga = 1u << long_lines_log2(a), Gb = 1u << long_lines_log2(b);
+  return ffts * (t[a] * (double)((b + Ga - 1) / Ga) + t[b] * (double)((a + Gb - 1) / Gb)) +
+         passes * 30.0 * (double)T;
+}
+
+// T = N1 * N2 with both factors 13-smooth in [2, 512]: the split of the
+// lowest estimated cost (*cost); 0 when none exists.
+static uint64_t long_split(uint64_t T, int ffts = 1, int passes = 2, double* cost = nullptr) {
+  const std::vector<double>& t = long_task_costs();
   uint64_t best_a = 0;
   double best = 1e300;
   for (uint64_t a = 2; a <= 512; ++a) {
-    if (T % a || T / a > 512 || T / a < 2) continue;
-    const uint64_t b = T / a;
-    const double score = 8.0 * ((4 - long_lines_log2(a)) + (4 - long_lines_log2(b))) +
-                         std::fabs(std::log((double)a) - std::log((double)b));
-    if (score < best) {
-      best = score;
+    if (T % a || T / a > 512 || T / a < 2 || t[a] == 0 || t[T / a] == 0) continue;
+    const double c = long_cost(T, a, ffts, passes);
+    if (c < best) {
+      best = c;
       best_a = a;
     }
   }
+  if (cost) *cost = best;
   return best_a;
 }
 
@@ -300,13 +348,18 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
     while (!smooth7(M)) ++M;
     uint64_t mlong = 0, a = 0;
     if (cta_bytes(M) > cta_cap && !clusters) {
-      // the smallest 7-smooth convolution length that splits into factors <= 512
-      for (uint64_t m = 2 * N - 1; !mlong && m <= 262144; ++m) {
-        if (!smooth7(m)) continue;
-        a = long_split(m);
-        if (a) {
+      // the 13-smooth convolution length in [2N - 1, 2.25 N] (and its split
+      // into factors <= 512) of the lowest estimated cost: a slightly longer
+      // convolution with fewer, larger-radix stages is often cheaper
+      double best = 1e300;
+      for (uint64_t m = 2 * N - 1; m <= 262144 && (m <= 9 * N / 4 || !mlong); ++m) {
+        if (!is_smooth13(m)) continue;
+        double c = 0;
+        const uint64_t am = long_split(m, 2, 3, &c);
+        if (am && c < best) {
+          best = c;
           mlong = m;
-          break;
+          a = am;
         }
       }
     }
