@@ -501,6 +501,17 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
         for (uint32_t a = 0; a < g.N1; ++a) tw.push_back(root_fwd((uint64_t)a * g.N2, g.M));
         g.tb = (uint32_t)tw.size();
         for (uint32_t c = 0; c < g.N2; ++c) tw.push_back(root_fwd(c, g.M));
+        if (g.blue) {
+          // chirp W_2N^q, q = a B + b, B = ceil(sqrt(2N))
+          const uint64_t twoN = 2ull * g.N;
+          uint64_t B = (uint64_t)std::ceil(std::sqrt((double)twoN));
+          while (B * B < twoN) ++B;
+          g.ca = (uint32_t)tw.size();
+          for (uint64_t a = 0; a * B < twoN; ++a) tw.push_back(root_fwd(a * B, twoN));
+          g.cb = (uint32_t)tw.size();
+          for (uint64_t b = 0; b < B; ++b) tw.push_back(root_fwd(b, twoN));
+          g.dCB = make_fastdiv((uint32_t)B);
+        }
         continue;
       }
       attach_stage_table(d.sch, tw, cache);

@@ -64,6 +64,8 @@ struct LongLenDesc {
   const c32* bhat;    // Bluestein: spectrum of the conjugate chirp / M, natural order
   uint32_t ta, tb;    // W_M^{a N2} (a < N1), W_M^b (b < N2): offsets into the twiddle table
   FastDiv dN2;
+  uint32_t ca, cb;    // Bluestein chirp: W_2N^{a B} (a < ceil(2N / B)), W_2N^b (b < B)
+  FastDiv dCB;        // B = ceil(sqrt(2N))
   LongSched s1, s2;   // schedules of N1 (columns) and N2 (rows)
 };
 
@@ -237,10 +239,18 @@ FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t t
 }
 
 // Chirp exp(-i pi n^2 / N) at n, n + D, n + 2D, ... : q = n^2 mod 2N kept
-// incrementally ((n + D)^2 = n^2 + 2nD + D^2); value() = W_2N^q.
+// incrementally ((n + D)^2 = n^2 + 2nD + D^2); value() = W_2N^q from the
+// length's two-level chirp table (q = a B + b: ca[a] * cb[b], both small
+// enough to stay in the read-only cache).
 struct ChirpWalk {
   uint32_t q, u, dsq, u2, twoN;
-  FFT_D void init(uint64_t n, uint32_t D, uint32_t N) {
+  const c32* ca;
+  const c32* cb;
+  FastDiv dB;
+  FFT_D void init(uint64_t n, uint32_t D, uint32_t N, const c32* tw, const LongLenDesc& d) {
+    ca = tw + d.ca;
+    cb = tw + d.cb;
+    dB = d.dCB;
     twoN = 2 * N;
     q = (uint32_t)((n * n) % twoN);
     u = (uint32_t)((2 * n * (uint64_t)D) % twoN);
@@ -255,7 +265,12 @@ struct ChirpWalk {
     u += u2;
     if (u >= twoN) u -= twoN;
   }
-  FFT_D c32 value() const { return twiddle_f32(q, twoN); }
+  FFT_D c32 value() const {
+    const uint32_t a = fdiv(q, dB), b = q - a * dB.d;
+    const float2 x = __ldg(reinterpret_cast<const float2*>(ca + a));
+    const float2 y = __ldg(reinterpret_cast<const float2*>(cb + b));
+    return cmul(c32{x.x, x.y}, c32{y.x, y.y});
+  }
 };
 
 FFT_D void copy_async(c32* dst, const c32* src, uint32_t n, uint32_t tid) {
@@ -329,7 +344,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
     if (c < N2) {
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N);
+      cw.init(n, S * N2, d.N, p.tw, d);
       c32* dp = X + i0 * P + l;
       for (uint32_t i = i0; i < N1 && n < d.N; i += S) {
         c32 v = *dp;
@@ -428,7 +443,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
       const float sc = d.scale;
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N);
+      cw.init(n, S * N2, d.N, p.tw, d);
       c32* dst = p.out + ln.base + n;
       const c32* sp = r + i0 * P + l;
       for (uint32_t n1 = i0; n1 < N1 && n < d.N; n1 += S) {
