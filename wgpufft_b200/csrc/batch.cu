@@ -86,8 +86,8 @@ static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
 // equal bytes, each copied in, transformed and copied out on its own.
 constexpr uint32_t kHostChunks = 8;
 // work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
-// cluster queues, [4 + ph] long-line phase ph; per chunk c of a host
-// execution, [8 + 4c] its CTA tasks and [9 + 4c + ph] its long phase ph
+// cluster queues; per chunk c of a host execution, [8 + 4c] its CTA tasks
+// (the long-line kernel takes its tasks in a static order and needs none)
 constexpr unsigned kBatchCounters = 8 + 4 * kHostChunks;
 
 struct BatchPlan {
@@ -105,7 +105,6 @@ struct BatchPlan {
   // long lines (k_long_pass): length descriptors, lines, and the tasks of
   // the column, row and Bluestein inverse-column phases, one launch each
   LongLenDesc* d_long_lens = nullptr;
-  LongLine* d_long_lines = nullptr;
   LongTask* d_long_tasks = nullptr;
   LongTask* d_long_tasks_chunked = nullptr;
   uint32_t long_first[3] = {0, 0, 0}, long_count[3] = {0, 0, 0};
@@ -150,7 +149,6 @@ struct BatchPlan {
     cudaFree(d_scratch);
     cudaFree(d_tw);
     cudaFree(d_long_lens);
-    cudaFree(d_long_lines);
     cudaFree(d_long_tasks);
     cudaFree(d_long_tasks_chunked);
     if (side) cudaStreamDestroy(side);
@@ -592,7 +590,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   // lines sorted by length index; CTA tasks reference contiguous runs.
   // Long lines get one task per column or row group in each of their
   // phases (1: columns, 2: rows, 3: Bluestein inverse columns).
-  std::vector<LongLine> long_lines;
+  uint64_t n_long_lines = 0;
   std::vector<LongTask> long_tasks[3];
   std::vector<uint32_t> long_task_chunk[3];
   uint64_t scratch_total = 0;
@@ -605,23 +603,23 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       const LongLenDesc& g = infos[li].lng;
       const uint32_t Gc = 1u << g.lgc, Gr = 1u << g.lgr;
       for (uint64_t line : lines) {
-        const uint32_t idx = (uint32_t)long_lines.size();
-        long_lines.push_back(LongLine{offsets[line], scratch_total, (uint32_t)li, 0});
+        const uint64_t lbase = offsets[line], lscr = scratch_total;
+        ++n_long_lines;
         scratch_total += g.M;
         bp->elems_long += lens_list[li];
         bp->lines_long += 1;
         const uint32_t ch = chunk_of[line];
         for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
-          long_tasks[0].push_back(LongTask{idx, g0});
+          long_tasks[0].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
           long_task_chunk[0].push_back(ch);
         }
         for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr) {
-          long_tasks[1].push_back(LongTask{idx, g0});
+          long_tasks[1].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
           long_task_chunk[1].push_back(ch);
         }
         if (g.blue)
           for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
-            long_tasks[2].push_back(LongTask{idx, g0});
+            long_tasks[2].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
             long_task_chunk[2].push_back(ch);
           }
       }
@@ -737,7 +735,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   if (!all.empty()) cudaMemcpy(bp->d_tasks, all.data(), all.size() * sizeof(BatchTask), cudaMemcpyHostToDevice);
   cudaMemcpy(bp->d_off, sorted_off.data(), sorted_off.size() * 8, cudaMemcpyHostToDevice);
   // long lines: descriptors (indexed like the length table), lines, tasks
-  if (!long_lines.empty()) {
+  if (n_long_lines) {
     std::vector<LongLenDesc> gl(infos.size());
     std::memset(gl.data(), 0, gl.size() * sizeof(LongLenDesc));
     for (size_t i = 0; i < infos.size(); ++i)
@@ -751,15 +749,12 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     }
     const bool okl =
         cudaMalloc(&bp->d_long_lens, gl.size() * sizeof(LongLenDesc)) == cudaSuccess &&
-        cudaMalloc(&bp->d_long_lines, long_lines.size() * sizeof(LongLine)) == cudaSuccess &&
         cudaMalloc(&bp->d_long_tasks, lt.size() * sizeof(LongTask)) == cudaSuccess &&
         cudaMalloc(&bp->d_long_tasks_chunked, ltc.size() * sizeof(LongTask)) == cudaSuccess &&
         cudaMalloc(&bp->d_scratch, scratch_total * 8) == cudaSuccess;
     if (!okl) return fail(B2F_ERR_RESOURCE_ALLOCATION, "batch long-line allocation failed");
     bp->scratch_bytes = scratch_total * 8;
     cudaMemcpy(bp->d_long_lens, gl.data(), gl.size() * sizeof(LongLenDesc), cudaMemcpyHostToDevice);
-    cudaMemcpy(bp->d_long_lines, long_lines.data(), long_lines.size() * sizeof(LongLine),
-               cudaMemcpyHostToDevice);
     cudaMemcpy(bp->d_long_tasks, lt.data(), lt.size() * sizeof(LongTask), cudaMemcpyHostToDevice);
     cudaMemcpy(bp->d_long_tasks_chunked, ltc.data(), ltc.size() * sizeof(LongTask), cudaMemcpyHostToDevice);
   }
@@ -774,7 +769,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     per_sm = std::max(per_sm, 1);
     bp->grid_cta = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm, bp->n_cta);
   }
-  if (!long_lines.empty()) {
+  if (n_long_lines) {
     bp->smem_long = (3 * (size_t)bp->long_cap + 2 * kLongTab) * 8;
     if (set_smem(k_long_pass, bp->smem_long) != cudaSuccess)
       return fail(B2F_ERR_DEVICE, "long-line kernel shared memory");
@@ -957,7 +952,6 @@ static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, vo
     lp.scratch = bp.d_scratch;
     lp.tw = bp.d_tw;
     lp.lens = bp.d_long_lens;
-    lp.lines = bp.d_long_lines;
     lp.cap = bp.long_cap;
     lp.inverse = bp.direction == B2F_INVERSE ? 1u : 0u;
     for (uint32_t ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
@@ -967,7 +961,6 @@ static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, vo
       lp.tasks = (chunk < 0 ? bp.d_long_tasks : bp.d_long_tasks_chunked) + bp.long_first[ph] + first;
       lp.ntasks = count;
       lp.phase = ph + 1;
-      lp.counter = bp.d_counters + (chunk < 0 ? 4 + ph : 9 + 4 * chunk + ph);
       const unsigned grid = (unsigned)std::min<uint64_t>(bp.grid_long, (count + kLongChunk - 1) / kLongChunk);
       k_long_pass<<<grid, kLongThreads, bp.smem_long, st>>>(lp);
       e = cudaGetLastError();

@@ -69,17 +69,16 @@ struct LongLenDesc {
   LongSched s1, s2;   // schedules of N1 (columns) and N2 (rows)
 };
 
-struct LongLine {
+// One task: G adjacent columns or rows of one line.  Self-contained, so
+// that the kernel can prefetch it with asynchronous copies (no dependent
+// load of a line record).
+struct LongTask {
   uint64_t base;     // complex offset of the line in the input and output buffers
   uint64_t scratch;  // complex offset of its scratch region (M values)
   uint32_t len;      // index into the length table
-  uint32_t pad;
+  uint32_t g0;       // first column (column passes) or row (row passes) of the task
 };
-
-struct LongTask {
-  uint32_t line;
-  uint32_t g0;  // first column (column passes) or row (row passes) of the task
-};
+static_assert(sizeof(LongTask) == 24, "task records are copied as three 8-byte words");
 
 struct LongParams {
   const c32* in;
@@ -87,13 +86,11 @@ struct LongParams {
   c32* scratch;
   const c32* tw;
   const LongLenDesc* lens;
-  const LongLine* lines;
   const LongTask* tasks;
   uint32_t ntasks;
   uint32_t phase;    // 1: column pass, 2: row pass, 3: Bluestein inverse columns
   uint32_t inverse;
   uint32_t cap;      // complex elements per shared-memory buffer
-  unsigned int* counter;
 };
 
 // cp.async of 8 bytes, zero-filled (nothing read) when !valid.
@@ -280,8 +277,9 @@ FFT_D void copy_async(c32* dst, const c32* src, uint32_t n, uint32_t tid) {
 // Issues the copies of one task into the landing buffer X (zero-filled
 // where the task has no data) and, with tables, of its length's twiddle
 // tables into the table area T.
-FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongLine& ln, uint32_t g0,
-                      uint32_t kind, c32* X, c32* T, bool tables, uint32_t tid) {
+FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongTask& ln, uint32_t kind,
+                      c32* X, c32* T, bool tables, uint32_t tid) {
+  const uint32_t g0 = ln.g0;
   const bool colk = kind == LP_COL || kind == LP_BCOL1 || kind == LP_BCOL3;
   if (tables) {
     const LongSched& sch = colk ? d.s1 : d.s2;
@@ -330,8 +328,9 @@ FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongLine&
 
 // Transforms the task whose data sits in X (W: the ping-pong partner, T:
 // its table area) and stores its results.  Ends without a barrier.
-FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLine& ln, uint32_t g0,
-                        uint32_t kind, c32* X, c32* W, const c32* T, uint32_t tid) {
+FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTask& ln, uint32_t kind,
+                        c32* X, c32* W, const c32* T, uint32_t tid) {
+  const uint32_t g0 = ln.g0;
   const bool inv = p.inverse != 0;
   const bool colk = kind == LP_COL || kind == LP_BCOL1 || kind == LP_BCOL3;
   const uint32_t lg = colk ? d.lgc : d.lgr, G = 1u << lg, P = G + 1;
@@ -462,67 +461,98 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongLin
   }
 }
 
-// Persistent kernel of one long-line phase.  Dynamic shared memory: two
-// landing buffers and one work buffer of p.cap complex values, then the two
-// table areas of kLongTab values (one per landing buffer).
+// Persistent kernel of one long-line phase.  CTA b takes the chunks of
+// kLongChunk consecutive tasks b, b + gridDim.x, b + 2 gridDim.x, ... (a
+// static round robin: neighbouring chunks cost about the same, and no work
+// claim is ever waited for).  While iteration k transforms the CTA's task
+// k, asynchronous copies run three stages ahead: the data and tables of
+// task k + 1 (into the other landing buffer), the length descriptor of
+// task k + 2 (a ring of three) and the record of task k + 3 (a ring of
+// four), committed as one group and waited for at the top of iteration
+// k + 1, so no descriptor load sits on the critical path.
+// Dynamic shared memory: two landing buffers and one work buffer of p.cap
+// complex values, then the two table areas of kLongTab values (one per
+// landing buffer).
 __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_constant__ LongParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ LongLenDesc s_len[2];
-  __shared__ LongLine s_line[2];
-  __shared__ uint32_t s_g0[2];
-  __shared__ uint32_t s_claim;
+  __shared__ LongLenDesc s_len[3];
+  __shared__ LongTask s_task[4];
+  static_assert(sizeof(LongLenDesc) % 8 == 0, "descriptors are copied as 8-byte words");
   c32* const base = reinterpret_cast<c32*>(smem_raw);
   c32* const work = base + 2 * p.cap;
   c32* const tab = base + 3 * p.cap;
   const uint32_t tid = threadIdx.x;
-  uint32_t held0 = 0xFFFFFFFFu, held1 = 0xFFFFFFFFu;  // length whose tables slot 0/1 holds
-  bool tables = false;  // the slot being staged needs its tables (same in every thread)
-  // descriptors of task t into slot
-  auto stage = [&](uint32_t t, uint32_t slot) {
-    const LongTask task = p.tasks[t];
-    const LongLine ln = p.lines[task.line];
-    const uint32_t held = slot ? held1 : held0;
-    tables = ln.len != held;
-    if (tables) copy_words(&s_len[slot], p.lens + ln.len, tid, kLongThreads);
-    if (slot) held1 = ln.len;
-    else held0 = ln.len;
-    if (tid == 0) {
-      s_line[slot] = ln;
-      s_g0[slot] = task.g0;
-    }
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  // the CTA's k-th task; kNone from the first one past the end (the
+  // sequence increases with k)
+  auto task_of = [&](uint32_t k) -> uint32_t {
+    const uint64_t t =
+        ((uint64_t)blockIdx.x + (uint64_t)(k / kLongChunk) * gridDim.x) * kLongChunk + k % kLongChunk;
+    return t < p.ntasks ? (uint32_t)t : kNone;
   };
-  auto issue = [&](uint32_t slot) {
-    const LongLenDesc& d = s_len[slot];
-    long_issue(p, d, s_line[slot], s_g0[slot], long_kind(p.phase, d.blue != 0), base + slot * p.cap,
-               tab + slot * kLongTab, tables, tid);
+  uint32_t held0 = kNone, held1 = kNone;        // length whose tables landing buffer 0/1 holds
+  uint32_t ring0 = kNone, ring1 = kNone, ring2 = kNone;  // length each descriptor slot holds
+  // record of task k into s_task[k % 4]
+  auto fetch_task = [&](uint32_t k) {
+    const uint32_t t = task_of(k);
+    if (t != kNone && tid < 3)
+      cp_async8_zfill(reinterpret_cast<uint64_t*>(&s_task[k & 3]) + tid,
+                      reinterpret_cast<const uint64_t*>(p.tasks + t) + tid, true);
   };
-  if (tid == 0) s_claim = atomicAdd(p.counter, 1u) * kLongChunk;
-  __syncthreads();
-  uint32_t t = s_claim;
-  uint32_t slot = 0;
-  if (t < p.ntasks) stage(t, 0);
-  __syncthreads();
-  if (t < p.ntasks) issue(0);
+  // length descriptor of task k (whose record has landed) into s_len[k % 3],
+  // unless that slot holds it already
+  auto fetch_len = [&](uint32_t k) {
+    if (task_of(k) == kNone) return;
+    const uint32_t len = s_task[k & 3].len, r = k % 3;
+    const uint32_t had = r == 0 ? ring0 : (r == 1 ? ring1 : ring2);
+    if (had == len) return;
+    if (r == 0) ring0 = len;
+    else if (r == 1) ring1 = len;
+    else ring2 = len;
+    const uint64_t* src = reinterpret_cast<const uint64_t*>(p.lens + len);
+    uint64_t* dst = reinterpret_cast<uint64_t*>(&s_len[r]);
+    for (uint32_t i = tid; i < sizeof(LongLenDesc) / 8; i += kLongThreads)
+      cp_async8_zfill(dst + i, src + i, true);
+  };
+  // data of task k (whose record and descriptor have landed) into landing
+  // buffer k % 2, with its length's tables when that buffer's differ
+  auto fetch_data = [&](uint32_t k) {
+    if (task_of(k) == kNone) return;
+    const LongTask& tk = s_task[k & 3];
+    const LongLenDesc& d = s_len[k % 3];
+    const uint32_t slot = k & 1;
+    const bool tables = tk.len != (slot ? held1 : held0);
+    if (slot) held1 = tk.len;
+    else held0 = tk.len;
+    long_issue(p, d, tk, long_kind(p.phase, d.blue != 0), base + slot * p.cap, tab + slot * kLongTab,
+               tables, tid);
+  };
+  fetch_task(0);
+  fetch_task(1);
+  fetch_task(2);
   cp_async_commit();
-  while (t < p.ntasks) {
-    __syncthreads();  // every thread is past the previous task's stores and has read s_claim
-    uint32_t tn = t + 1;
-    if (tn % kLongChunk == 0 || tn >= p.ntasks) {  // next chunk
-      if (tid == 0) s_claim = atomicAdd(p.counter, 1u) * kLongChunk;
-      __syncthreads();
-      tn = s_claim;
-    }
-    if (tn < p.ntasks) stage(tn, slot ^ 1);
-    __syncthreads();
-    if (tn < p.ntasks) issue(slot ^ 1);
+  cp_async_wait<0>();
+  __syncthreads();
+  fetch_len(0);
+  fetch_len(1);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  fetch_data(0);
+  cp_async_commit();
+#pragma unroll 1
+  for (uint32_t k = 0; task_of(k) != kNone; ++k) {
+    cp_async_wait<0>();
+    __syncthreads();  // task k's data, k + 1's descriptor and k + 2's record have landed,
+                      // and every thread is past task k - 1
+    fetch_data(k + 1);
+    fetch_len(k + 2);
+    fetch_task(k + 3);
     cp_async_commit();
-    cp_async_wait<1>();  // this thread's copies of the current task have landed
-    __syncthreads();
-    const LongLenDesc& d = s_len[slot];
-    long_compute(p, d, s_line[slot], s_g0[slot], long_kind(p.phase, d.blue != 0),
-                 base + slot * p.cap, work, tab + slot * kLongTab, tid);
-    slot ^= 1;
-    t = tn;
+    const LongLenDesc& d = s_len[k % 3];
+    const uint32_t slot = k & 1;
+    long_compute(p, d, s_task[k & 3], long_kind(p.phase, d.blue != 0), base + slot * p.cap, work,
+                 tab + slot * kLongTab, tid);
   }
   cp_async_wait<0>();
 }
