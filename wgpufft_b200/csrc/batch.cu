@@ -86,8 +86,8 @@ static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
 // equal bytes, each copied in, transformed and copied out on its own.
 constexpr uint32_t kHostChunks = 8;
 // work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
-// cluster queues; per chunk c of a host execution, [8 + 4c] its CTA tasks
-// (the long-line kernel takes its tasks in a static order and needs none)
+// cluster queues, [4 + ph] long-line phase ph; per chunk c of a host
+// execution, [8 + 4c] its CTA tasks and [9 + 4c + ph] its long phase ph
 constexpr unsigned kBatchCounters = 8 + 4 * kHostChunks;
 
 struct BatchPlan {
@@ -961,6 +961,7 @@ static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, vo
       lp.tasks = (chunk < 0 ? bp.d_long_tasks : bp.d_long_tasks_chunked) + bp.long_first[ph] + first;
       lp.ntasks = count;
       lp.phase = ph + 1;
+      lp.counter = bp.d_counters + (chunk < 0 ? 4 + ph : 9 + 4 * chunk + ph);
       const unsigned grid = (unsigned)std::min<uint64_t>(bp.grid_long, (count + kLongChunk - 1) / kLongChunk);
       k_long_pass<<<grid, kLongThreads, bp.smem_long, st>>>(lp);
       e = cudaGetLastError();

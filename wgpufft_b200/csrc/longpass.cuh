@@ -91,6 +91,7 @@ struct LongParams {
   uint32_t phase;    // 1: column pass, 2: row pass, 3: Bluestein inverse columns
   uint32_t inverse;
   uint32_t cap;      // complex elements per shared-memory buffer
+  unsigned int* counter;  // work queue: chunks of kLongChunk tasks handed out in order
 };
 
 // cp.async of 8 bytes, zero-filled (nothing read) when !valid.
@@ -461,15 +462,17 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
   }
 }
 
-// Persistent kernel of one long-line phase.  CTA b takes the chunks of
-// kLongChunk consecutive tasks b, b + gridDim.x, b + 2 gridDim.x, ... (a
-// static round robin: neighbouring chunks cost about the same, and no work
-// claim is ever waited for).  While iteration k transforms the CTA's task
-// k, asynchronous copies run three stages ahead: the data and tables of
-// task k + 1 (into the other landing buffer), the length descriptor of
-// task k + 2 (a ring of three) and the record of task k + 3 (a ring of
-// four), committed as one group and waited for at the top of iteration
-// k + 1, so no descriptor load sits on the critical path.
+// Persistent kernel of one long-line phase.  CTAs take chunks of
+// kLongChunk consecutive tasks from a work queue (one atomicAdd per
+// chunk), claimed a chunk ahead: the claim for the CTA's chunk c + 1 is
+// issued when it starts using chunk c and its result is stored after that
+// iteration's transform, so the atomic's latency is hidden too.  While
+// iteration k transforms the CTA's task k, asynchronous copies run three
+// stages ahead: the data and tables of task k + 1 (into the other landing
+// buffer), the length descriptor of task k + 2 (a ring of three) and the
+// record of task k + 3 (a ring of four), committed as one group and
+// waited for at the top of iteration k + 1, so no descriptor load sits on
+// the critical path.
 // Dynamic shared memory: two landing buffers and one work buffer of p.cap
 // complex values, then the two table areas of kLongTab values (one per
 // landing buffer).
@@ -477,19 +480,24 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ LongLenDesc s_len[3];
   __shared__ LongTask s_task[4];
+  __shared__ uint32_t s_chunk[4];  // first task of the CTA's chunk c, at c % 4
   static_assert(sizeof(LongLenDesc) % 8 == 0, "descriptors are copied as 8-byte words");
   c32* const base = reinterpret_cast<c32*>(smem_raw);
   c32* const work = base + 2 * p.cap;
   c32* const tab = base + 3 * p.cap;
   const uint32_t tid = threadIdx.x;
   constexpr uint32_t kNone = 0xFFFFFFFFu;
-  // the CTA's k-th task; kNone from the first one past the end (the
-  // sequence increases with k)
+  // the CTA's k-th task (its chunk claimed and visible); kNone from the
+  // first one past the end (the queue hands out chunks in increasing order)
   auto task_of = [&](uint32_t k) -> uint32_t {
-    const uint64_t t =
-        ((uint64_t)blockIdx.x + (uint64_t)(k / kLongChunk) * gridDim.x) * kLongChunk + k % kLongChunk;
+    const uint64_t t = (uint64_t)s_chunk[(k / kLongChunk) & 3] + k % kLongChunk;
     return t < p.ntasks ? (uint32_t)t : kNone;
   };
+  if (tid == 0) {
+    s_chunk[0] = atomicAdd(p.counter, 1u) * kLongChunk;
+    s_chunk[1] = atomicAdd(p.counter, 1u) * kLongChunk;
+  }
+  __syncthreads();
   uint32_t held0 = kNone, held1 = kNone;        // length whose tables landing buffer 0/1 holds
   uint32_t ring0 = kNone, ring1 = kNone, ring2 = kNone;  // length each descriptor slot holds
   // record of task k into s_task[k % 4]
@@ -545,6 +553,9 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
     cp_async_wait<0>();
     __syncthreads();  // task k's data, k + 1's descriptor and k + 2's record have landed,
                       // and every thread is past task k - 1
+    // task k + 3 opens chunk c = (k + 3) / kLongChunk: claim chunk c + 1
+    const bool claim = tid == 0 && (k + 3) % kLongChunk == 0;
+    const uint32_t claimed = claim ? atomicAdd(p.counter, 1u) * kLongChunk : 0u;
     fetch_data(k + 1);
     fetch_len(k + 2);
     fetch_task(k + 3);
@@ -553,6 +564,8 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
     const uint32_t slot = k & 1;
     long_compute(p, d, s_task[k & 3], long_kind(p.phase, d.blue != 0), base + slot * p.cap, work,
                  tab + slot * kLongTab, tid);
+    // first read at iteration k + 4, after the barriers between
+    if (claim) s_chunk[((k + 3) / kLongChunk + 1) & 3] = claimed;
   }
   cp_async_wait<0>();
 }
