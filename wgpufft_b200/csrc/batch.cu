@@ -677,6 +677,23 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     if (bp->cta_ccount[c] == 0) bp->cta_cfirst[c] = (uint32_t)i;
     ++bp->cta_ccount[c];
   }
+  // within each phase, the smooth lines' tasks before the Bluestein lines'
+  // (one code path at a time keeps the instruction cache warm)
+  for (int ph = 0; ph < 3; ++ph) {
+    std::vector<size_t> idx(long_tasks[ph].size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+      return infos[long_tasks[ph][a].len].lng.blue < infos[long_tasks[ph][b].len].lng.blue;
+    });
+    std::vector<LongTask> t(idx.size());
+    std::vector<uint32_t> c(idx.size());
+    for (size_t i = 0; i < idx.size(); ++i) {
+      t[i] = long_tasks[ph][idx[i]];
+      c[i] = long_task_chunk[ph][idx[i]];
+    }
+    long_tasks[ph].swap(t);
+    long_task_chunk[ph].swap(c);
+  }
   // long tasks of each phase chunk by chunk, likewise
   std::vector<LongTask> long_chunked[3];
   for (int ph = 0; ph < 3; ++ph) {

@@ -39,7 +39,9 @@ constexpr uint32_t kLongThreads = 256;
 constexpr int kLongMaxStages = 10;  // pass lengths <= 512
 constexpr uint32_t kLongChunk = 4;  // consecutive tasks per work-queue claim
 // table area of one landing buffer (complex values): stage twiddles of the
-// pass (length - 1 <= 511), W_M^{a N2} (a < N1 <= 512), W_M^b (b < N2 <= 512)
+// pass (length - 1 <= 511), W_M^{a N2} (a < N1 <= 512), W_M^b (b < N2 <= 512);
+// the Bluestein inverse column pass holds the chirp tables W_2N^{a B} and
+// W_2N^b (B = ceil(sqrt(2N)) <= 512) where the last two are
 constexpr uint32_t kTabSt = 0, kTabTa = 512, kTabTb = 1024;
 constexpr uint32_t kLongTab = 1536;
 
@@ -237,17 +239,18 @@ FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t t
 }
 
 // Chirp exp(-i pi n^2 / N) at n, n + D, n + 2D, ... : q = n^2 mod 2N kept
-// incrementally ((n + D)^2 = n^2 + 2nD + D^2); value() = W_2N^q from the
-// length's two-level chirp table (q = a B + b: ca[a] * cb[b], both small
-// enough to stay in the read-only cache).
+// incrementally ((n + D)^2 = n^2 + 2nD + D^2); W_2N^q from the length's
+// two-level chirp table (q = a B + b: ca[a] * cb[b]), read through the
+// read-only cache (value_ldg) or from a shared-memory copy (value).
 struct ChirpWalk {
   uint32_t q, u, dsq, u2, twoN;
   const c32* ca;
   const c32* cb;
   FastDiv dB;
-  FFT_D void init(uint64_t n, uint32_t D, uint32_t N, const c32* tw, const LongLenDesc& d) {
-    ca = tw + d.ca;
-    cb = tw + d.cb;
+  FFT_D void init(uint64_t n, uint32_t D, uint32_t N, const c32* ta, const c32* tb,
+                  const LongLenDesc& d) {
+    ca = ta;
+    cb = tb;
     dB = d.dCB;
     twoN = 2 * N;
     q = (uint32_t)((n * n) % twoN);
@@ -263,11 +266,15 @@ struct ChirpWalk {
     u += u2;
     if (u >= twoN) u -= twoN;
   }
-  FFT_D c32 value() const {
+  FFT_D c32 value_ldg() const {
     const uint32_t a = fdiv(q, dB), b = q - a * dB.d;
     const float2 x = __ldg(reinterpret_cast<const float2*>(ca + a));
     const float2 y = __ldg(reinterpret_cast<const float2*>(cb + b));
     return cmul(c32{x.x, x.y}, c32{y.x, y.y});
+  }
+  FFT_D c32 value() const {
+    const uint32_t a = fdiv(q, dB), b = q - a * dB.d;
+    return cmul(ca[a], cb[b]);
   }
 };
 
@@ -289,6 +296,10 @@ FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongTask&
     if (kind == LP_COL || kind == LP_BCOL1 || kind == LP_BMID) {
       copy_async(T + kTabTa, p.tw + d.ta, d.N1, tid);
       copy_async(T + kTabTb, p.tw + d.tb, d.N2, tid);
+    } else if (kind == LP_BCOL3) {
+      // the chirp tables (ceil(2N / B) <= B <= 512 values each) in their place
+      copy_async(T + kTabTa, p.tw + d.ca, (2 * d.N + d.dCB.d - 1) / d.dCB.d, tid);
+      copy_async(T + kTabTb, p.tw + d.cb, d.dCB.d, tid);
     }
   }
   if (colk) {
@@ -344,12 +355,12 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
     if (c < N2) {
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N, p.tw, d);
+      cw.init(n, S * N2, d.N, p.tw + d.ca, p.tw + d.cb, d);
       c32* dp = X + i0 * P + l;
       for (uint32_t i = i0; i < N1 && n < d.N; i += S) {
         c32 v = *dp;
         if (inv) v.im = -v.im;
-        *dp = cmul(v, cw.value());
+        *dp = cmul(v, cw.value_ldg());
         cw.step();
         n += S * N2;
         dp += S * P;
@@ -443,7 +454,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
       const float sc = d.scale;
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N, p.tw, d);
+      cw.init(n, S * N2, d.N, T + kTabTa, T + kTabTb, d);
       c32* dst = p.out + ln.base + n;
       const c32* sp = r + i0 * P + l;
       for (uint32_t n1 = i0; n1 < N1 && n < d.N; n1 += S) {
