@@ -788,10 +788,12 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   }
   if (n_long_lines) {
     bp->smem_long = (3 * (size_t)bp->long_cap + 2 * kLongTab) * 8;
-    if (set_smem(k_long_pass, bp->smem_long) != cudaSuccess)
+    if (set_smem(k_long_pass<1>, bp->smem_long) != cudaSuccess ||
+        set_smem(k_long_pass<2>, bp->smem_long) != cudaSuccess ||
+        set_smem(k_long_pass<3>, bp->smem_long) != cudaSuccess)
       return fail(B2F_ERR_DEVICE, "long-line kernel shared memory");
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_long_pass, kLongThreads, bp->smem_long);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_long_pass<2>, kLongThreads, bp->smem_long);
     per_sm = std::max(per_sm, 1);
     uint32_t most = std::max(bp->long_count[0], std::max(bp->long_count[1], bp->long_count[2]));
     bp->grid_long = (unsigned)std::min<uint64_t>((uint64_t)nsm * per_sm,
@@ -980,7 +982,9 @@ static void launch_long(const BatchPlan& bp, cudaStream_t st, const void* in, vo
       lp.phase = ph + 1;
       lp.counter = bp.d_counters + (chunk < 0 ? 4 + ph : 9 + 4 * chunk + ph);
       const unsigned grid = (unsigned)std::min<uint64_t>(bp.grid_long, (count + kLongChunk - 1) / kLongChunk);
-      k_long_pass<<<grid, kLongThreads, bp.smem_long, st>>>(lp);
+      if (ph == 0) k_long_pass<1><<<grid, kLongThreads, bp.smem_long, st>>>(lp);
+      else if (ph == 1) k_long_pass<2><<<grid, kLongThreads, bp.smem_long, st>>>(lp);
+      else k_long_pass<3><<<grid, kLongThreads, bp.smem_long, st>>>(lp);
       e = cudaGetLastError();
     }
   }

@@ -484,9 +484,11 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
 // record of task k + 3 (a ring of four), committed as one group and
 // waited for at the top of iteration k + 1, so no descriptor load sits on
 // the critical path.
-// Dynamic shared memory: two landing buffers and one work buffer of p.cap
-// complex values, then the two table areas of kLongTab values (one per
-// landing buffer).
+// One instantiation per phase PH (= p.phase), so each holds only the code
+// of its two task kinds.  Dynamic shared memory: two landing buffers and
+// one work buffer of p.cap complex values, then the two table areas of
+// kLongTab values (one per landing buffer).
+template <uint32_t PH>
 __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_constant__ LongParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ LongLenDesc s_len[3];
@@ -543,7 +545,7 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
     const bool tables = tk.len != (slot ? held1 : held0);
     if (slot) held1 = tk.len;
     else held0 = tk.len;
-    long_issue(p, d, tk, long_kind(p.phase, d.blue != 0), base + slot * p.cap, tab + slot * kLongTab,
+    long_issue(p, d, tk, long_kind(PH, d.blue != 0), base + slot * p.cap, tab + slot * kLongTab,
                tables, tid);
   };
   fetch_task(0);
@@ -573,7 +575,7 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
     cp_async_commit();
     const LongLenDesc& d = s_len[k % 3];
     const uint32_t slot = k & 1;
-    long_compute(p, d, s_task[k & 3], long_kind(p.phase, d.blue != 0), base + slot * p.cap, work,
+    long_compute(p, d, s_task[k & 3], long_kind(PH, d.blue != 0), base + slot * p.cap, work,
                  tab + slot * kLongTab, tid);
     // first read at iteration k + 4, after the barriers between
     if (claim) s_chunk[((k + 3) / kLongChunk + 1) & 3] = claimed;
