@@ -677,14 +677,18 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     if (bp->cta_ccount[c] == 0) bp->cta_cfirst[c] = (uint32_t)i;
     ++bp->cta_ccount[c];
   }
-  // within each phase, the smooth lines' tasks before the Bluestein lines'
-  // (one code path at a time keeps the instruction cache warm)
+  // within each phase, the smooth lines' tasks before the Bluestein lines',
+  // and within each kind by the length of the pass (N1 for the column
+  // phases, N2 for the rows): consecutive tasks run the same code, which
+  // keeps the instruction cache warm
   for (int ph = 0; ph < 3; ++ph) {
     std::vector<size_t> idx(long_tasks[ph].size());
     for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-      return infos[long_tasks[ph][a].len].lng.blue < infos[long_tasks[ph][b].len].lng.blue;
-    });
+    auto key = [&](size_t i) {
+      const LongLenDesc& g = infos[long_tasks[ph][i].len].lng;
+      return std::make_pair(g.blue, ph == 1 ? g.N2 : g.N1);
+    };
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return key(a) < key(b); });
     std::vector<LongTask> t(idx.size());
     std::vector<uint32_t> c(idx.size());
     for (size_t i = 0; i < idx.size(); ++i) {
