@@ -36,6 +36,8 @@
 namespace b2f {
 
 constexpr uint32_t kLongThreads = 256;
+constexpr uint32_t kLongThreadsLog2 = 8;
+static_assert(kLongThreads == 1u << kLongThreadsLog2, "thread count is a power of two");
 constexpr int kLongMaxStages = 10;  // pass lengths <= 512
 constexpr uint32_t kLongChunk = 4;  // consecutive tasks per work-queue claim
 // table area of one landing buffer (complex values): stage twiddles of the
@@ -321,19 +323,18 @@ FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongTask&
       dp += S * P;
     }
   } else {
-    // rows g0..g0+G-1 of the scratch: warp w copies rows w, w+8, ...
-    const uint32_t lg = d.lgr, G = 1u << lg, P = G + 1;
+    // rows g0..g0+G-1 of the scratch: kLongThreads / G threads per row
+    // (a half-warp, a warp or two), each a run of consecutive values
+    const uint32_t lg = d.lgr, P = (1u << lg) + 1;
     const uint32_t N2 = d.N2, N1 = d.N1;
-    const uint32_t w = tid >> 5, lane = tid & 31;
-    for (uint32_t r = w; r < G; r += kLongThreads / 32) {
-      const bool ok = g0 + r < N1;
-      const c32* row = p.scratch + ln.scratch + (uint64_t)(ok ? g0 + r : 0) * N2;
-      c32* dp = X + lane * P + r;
+    const uint32_t tpr = kLongThreads >> lg, r = tid >> (kLongThreadsLog2 - lg), lane = tid & (tpr - 1);
+    const bool ok = g0 + r < N1;
+    const c32* row = p.scratch + ln.scratch + (uint64_t)(ok ? g0 + r : 0) * N2;
+    c32* dp = X + lane * P + r;
 #pragma unroll 4
-      for (uint32_t n2 = lane; n2 < N2; n2 += 32) {
-        cp_async8_zfill(dp, row + n2, ok);
-        dp += 32 * P;
-      }
+    for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
+      cp_async8_zfill(dp, row + n2, ok);
+      dp += tpr * P;
     }
   }
 }
@@ -435,17 +436,17 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
   }
   // stores
   if (kind == LP_BMID) {
-    // scratch row k1 = g0 + r, position n2: V * W_M^{n2 k1} (warp w writes rows w, w+8, ...)
-    const uint32_t w = tid >> 5, lane = tid & 31;
-    for (uint32_t rr = w; rr < G; rr += kLongThreads / 32) {
-      const uint32_t k1 = g0 + rr;
-      if (k1 >= N1) break;
+    // scratch row k1 = g0 + rr, position n2: V * W_M^{n2 k1}
+    // (kLongThreads / G threads per row, each a run of consecutive values)
+    const uint32_t tpr = kLongThreads >> lg, rr = tid >> (kLongThreadsLog2 - lg), lane = tid & (tpr - 1);
+    const uint32_t k1 = g0 + rr;
+    if (k1 < N1) {
       c32* row = p.scratch + ln.scratch + (uint64_t)k1 * N2;
       const c32* sp = r + lane * P + rr;
 #pragma unroll 4
-      for (uint32_t n2 = lane; n2 < N2; n2 += 32) {
+      for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
         row[n2] = cmul(*sp, tw_two(T, kTabTa, kTabTb, n2 * k1, d.dN2));
-        sp += 32 * P;
+        sp += tpr * P;
       }
     }
   } else {  // LP_BCOL3: out[n] = conj(Y[n]) * chirp(n), n = N2 n1 + g0 + l < N
