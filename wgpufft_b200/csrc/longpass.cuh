@@ -40,6 +40,10 @@ constexpr uint32_t kLongThreadsLog2 = 8;
 static_assert(kLongThreads == 1u << kLongThreadsLog2, "thread count is a power of two");
 constexpr int kLongMaxStages = 10;  // pass lengths <= 512
 constexpr uint32_t kLongChunk = 4;  // consecutive tasks per work-queue claim
+// k_long_pass claims the first two chunks before its loop and every later
+// one when the chunk before it opens (three tasks ahead): that covers every
+// chunk only when a chunk holds at least three tasks
+static_assert(kLongChunk >= 3, "the prologue claims chunks 0 and 1 only");
 // table area of one landing buffer (complex values): stage twiddles of the
 // pass (length - 1 <= 511), W_M^{a N2} (a < N1 <= 512), W_M^b (b < N2 <= 512);
 // the Bluestein inverse column pass holds the chirp tables W_2N^{a B} and
