@@ -944,18 +944,25 @@ static b2f_status run_batch(const BatchPlan& bp, cudaStream_t st, const void* in
       e = cudaLaunchKernelEx(&cfg, k_batch_cluster<kClusterBig>, pb, bp.buf_cl);
     }
   }
+  // without cluster lines, the CTA queue runs on the forked stream,
+  // concurrently with the long-line phases (no line is in both)
+  const bool cta_side = run_cta && !run_cl && !sequential && (parts & 4) && bp.lines_long;
+  if (e == cudaSuccess && cta_side) {
+    e = cudaEventRecord(bp.fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(bp.side, bp.fork, 0);
+  }
   if (e == cudaSuccess && run_cta) {
     BatchParams pt = p;
     pt.tasks = bp.d_tasks;
     pt.ntasks = bp.n_cta;
     pt.counter = bp.d_counters;
-    k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, st>>>(pt, bp.buf_cta);
+    k_batch_cta<<<bp.grid_cta, kCtaThreads, bp.smem_cta, cta_side ? bp.side : st>>>(pt, bp.buf_cta);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && (parts & 4) && bp.lines_long) {
     launch_long(bp, st, in, out, -1, &e);
   }
-  if (e == cudaSuccess && run_cl && !sequential) {
+  if (e == cudaSuccess && ((run_cl && !sequential) || cta_side)) {
     e = cudaEventRecord(bp.join, bp.side);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bp.join, 0);
   }
