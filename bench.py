@@ -10,7 +10,7 @@ flush is needed between steps).  One step = one batched launch over all
     execute_checked per line (what a caller of the reference's plan API does);
   - e2e: the batched step through the public API with the input copied from
     pinned host memory and the output copied back inside the timed region
-    (b2f_batch_execute_host: 8 chunks whose copies overlap the transforms);
+    (b2f_batch_execute_host: ~32 MiB chunks whose copies overlap the transforms);
   - roofline: the long-line kernel (k_long_pass: the column, row and
     Bluestein passes of every line too long for one CTA, which hold 97% of
     the points), timed alone; achieved algorithmic GB/s (16 B per complex

@@ -214,7 +214,7 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const v
                                    uint64_t in_bytes, void* out, uint64_t out_bytes,
                                    uint32_t parts, int32_t sequential);
 /* b2f_batch_execute from and to host memory: the lines are cut, in offset
- * order, into 8 chunks of about equal bytes, and chunk c's copy in
+ * order, into chunks of about 32 MiB (at most 32), and chunk c's copy in
  * (host_in -> dev_in), transform (dev_in -> dev_out) and copy out
  * (dev_out -> host_out) overlap the other chunks' on three internal
  * streams; `stream` orders the whole call with the caller's work (the call

@@ -82,9 +82,12 @@ static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
 }
 
 // Host-buffer execution (b2f_batch_execute_host) pipelines the lines in
-// kHostChunks chunks: contiguous runs of lines (in offset order) of about
-// equal bytes, each copied in, transformed and copied out on its own.
-constexpr uint32_t kHostChunks = 8;
+// chunks: contiguous runs of lines (in offset order) of about equal bytes,
+// about kHostChunkBytes each and at most kHostChunks, each copied in,
+// transformed and copied out on its own (smaller chunks shorten the
+// pipeline's fill and drain, which are all that the copies do not hide).
+constexpr uint32_t kHostChunks = 32;
+constexpr uint64_t kHostChunkBytes = 32ull << 20;
 // work-queue counters, zeroed by every execute: [0] CTA queue, [1] and [2]
 // cluster queues, [4 + ph] long-line phase ph; per chunk c of a host
 // execution, [8 + 4c] its CTA tasks and [9 + 4c + ph] its long phase ph
@@ -111,6 +114,7 @@ struct BatchPlan {
   // chunks of host execution: element ranges [chunk_lo, chunk_hi) of the
   // buffers, and each chunk's tasks (CTA queue; long phases, relative to
   // long_first) -- every task list is ordered by chunk
+  uint32_t n_chunks = 1;  // chunks in use (<= kHostChunks)
   uint64_t chunk_lo[kHostChunks] = {}, chunk_hi[kHostChunks] = {};
   uint32_t cta_cfirst[kHostChunks] = {}, cta_ccount[kHostChunks] = {};
   uint32_t long_cfirst[3][kHostChunks] = {}, long_ccount[3][kHostChunks] = {};
@@ -571,10 +575,13 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     uint64_t total = 0, acc = 0;
     for (uint64_t i = 0; i < nlines; ++i) total += lengths[i];
     for (uint32_t c = 0; c < kHostChunks; ++c) bp->chunk_lo[c] = bp->chunk_hi[c] = 0;
+    bp->n_chunks = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(kHostChunks, (total * 8 + kHostChunkBytes - 1) / kHostChunkBytes));
+    const uint32_t K = bp->n_chunks;
     bool seen[kHostChunks] = {};
     for (uint64_t i = 0; i < nlines; ++i) {
       const uint64_t l = order[i];
-      const uint32_t c = (uint32_t)std::min<uint64_t>(kHostChunks - 1, acc * kHostChunks / total);
+      const uint32_t c = (uint32_t)std::min<uint64_t>(K - 1, acc * K / total);
       chunk_of[l] = c;
       if (!seen[c]) bp->chunk_lo[c] = offsets[l];
       seen[c] = true;
@@ -585,8 +592,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
   // tasks: CTA tasks (groups of G lines of one length and one chunk),
   // cluster tasks (one line each)
   std::vector<uint64_t> sorted_off;
-  std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks;
-  std::vector<double> cta_cost, cl_cost, big_cost;
+  std::vector<BatchTask> cta_tasks, cl_tasks, big_tasks, cta_ch_tasks;
+  std::vector<double> cta_cost, cl_cost, big_cost, cta_ch_cost;
   // lines sorted by length index; CTA tasks reference contiguous runs.
   // Long lines get one task per column or row group in each of their
   // phases (1: columns, 2: rows, 3: Bluestein inverse columns).
@@ -625,36 +632,51 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
       }
       continue;
     }
-    std::vector<uint64_t> ls = lines;  // grouped by chunk: a task's lines share one
+    // the length's lines in chunk order, their offsets stored once; the
+    // whole-batch tasks take runs of up to G of them, the host-execution
+    // tasks runs of up to G within one chunk
+    std::vector<uint64_t> ls = lines;
     std::stable_sort(ls.begin(), ls.end(),
                      [&](uint64_t a, uint64_t b) { return chunk_of[a] < chunk_of[b]; });
+    const uint32_t first = (uint32_t)sorted_off.size();
+    for (uint64_t l : ls) sorted_off.push_back(offsets[l]);
+    auto make = [&](size_t s, size_t e, uint32_t ch) {
+      BatchTask t;
+      t.len = (uint32_t)li;
+      t.first = first + (uint32_t)s;
+      t.count = (uint32_t)(e - s);
+      t.pad = ch;  // chunk (not read by the kernels)
+      return t;
+    };
+    if (cl) {
+      for (size_t s = 0; s < ls.size(); ++s) {
+        const BatchTask t = make(s, s + 1, chunk_of[ls[s]]);
+        if (d.P == kClusterBig) {
+          big_tasks.push_back(t);
+          big_cost.push_back(infos[li].cost);
+        } else {
+          cl_tasks.push_back(t);
+          cl_cost.push_back(infos[li].cost);
+        }
+        bp->lines_cl += 1;
+        bp->elems_cl += lens_list[li];
+      }
+      continue;
+    }
+    for (size_t s = 0; s < ls.size(); s += d.G) {
+      const BatchTask t = make(s, std::min<size_t>(ls.size(), s + d.G), 0);
+      cta_tasks.push_back(t);
+      cta_cost.push_back(infos[li].cost * t.count);
+      bp->lines_cta += t.count;
+      bp->elems_cta += lens_list[li] * t.count;
+    }
     for (size_t s = 0; s < ls.size();) {
       const uint32_t ch = chunk_of[ls[s]];
       size_t e = s;
-      while (e < ls.size() && chunk_of[ls[e]] == ch && e - s < (cl ? 1u : d.G)) ++e;
-      BatchTask t;
-      t.len = (uint32_t)li;
-      t.first = (uint32_t)sorted_off.size();
-      t.count = (uint32_t)(e - s);
-      t.pad = ch;  // chunk (not read by the kernels)
-      for (uint32_t c = 0; c < t.count; ++c) sorted_off.push_back(offsets[ls[s + c]]);
+      while (e < ls.size() && chunk_of[ls[e]] == ch && e - s < d.G) ++e;
+      cta_ch_tasks.push_back(make(s, e, ch));
+      cta_ch_cost.push_back(infos[li].cost * (double)(e - s));
       s = e;
-      if (cl && d.P == kClusterBig) {
-        big_tasks.push_back(t);
-        big_cost.push_back(infos[li].cost);
-        bp->lines_cl += 1;
-        bp->elems_cl += lens_list[li];
-      } else if (cl) {
-        cl_tasks.push_back(t);
-        cl_cost.push_back(infos[li].cost);
-        bp->lines_cl += 1;
-        bp->elems_cl += lens_list[li];
-      } else {
-        cta_tasks.push_back(t);
-        cta_cost.push_back(infos[li].cost * t.count);
-        bp->lines_cta += t.count;
-        bp->elems_cta += lens_list[li] * t.count;
-      }
     }
   }
   // longest first (the queue hands them out in order)
@@ -667,9 +689,9 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     t.swap(out);
   };
   sort_by_cost(cta_tasks, cta_cost);
-  // the same tasks chunk by chunk (longest first within each), for host
-  // execution; the whole-batch queue keeps the global longest-first order
-  std::vector<BatchTask> cta_chunked = cta_tasks;
+  // the host-execution tasks chunk by chunk (longest first within each)
+  sort_by_cost(cta_ch_tasks, cta_ch_cost);
+  std::vector<BatchTask> cta_chunked = cta_ch_tasks;
   std::stable_sort(cta_chunked.begin(), cta_chunked.end(),
                    [](const BatchTask& a, const BatchTask& b) { return a.pad < b.pad; });
   for (size_t i = 0; i < cta_chunked.size(); ++i) {
@@ -1054,17 +1076,17 @@ static b2f_status run_batch_host(const BatchPlan& bp, cudaStream_t st, const voi
   for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(bp.hs[i], bp.hev_start, 0);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(bp.d_counters, 0, kBatchCounters * sizeof(unsigned int), sc);
-  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+  for (uint32_t c = 0; c < bp.n_chunks && e == cudaSuccess; ++c) {
     const uint64_t lo = bp.chunk_lo[c] * 8, n = (bp.chunk_hi[c] - bp.chunk_lo[c]) * 8;
     if (n) e = cudaMemcpyAsync((char*)dev_in + lo, (const char*)host_in + lo, n, cudaMemcpyHostToDevice, sin);
     if (e == cudaSuccess) e = cudaEventRecord(bp.hev_in[c], sin);
   }
-  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+  for (uint32_t c = 0; c < bp.n_chunks && e == cudaSuccess; ++c) {
     e = cudaStreamWaitEvent(sc, bp.hev_in[c], 0);
     if (e == cudaSuccess) e = run_chunk(bp, sc, dev_in, dev_out, (int)c);
     if (e == cudaSuccess) e = cudaEventRecord(bp.hev_c[c], sc);
   }
-  for (uint32_t c = 0; c < kHostChunks && e == cudaSuccess; ++c) {
+  for (uint32_t c = 0; c < bp.n_chunks && e == cudaSuccess; ++c) {
     const uint64_t lo = bp.chunk_lo[c] * 8, n = (bp.chunk_hi[c] - bp.chunk_lo[c]) * 8;
     e = cudaStreamWaitEvent(sout, bp.hev_c[c], 0);
     if (e == cudaSuccess && n)
