@@ -130,6 +130,8 @@ def test_batch_execute_host_matches_device_execute(cuda, lengths):
     # chunked copy-in / transform / copy-out: the same bits as the
     # device-resident execution, in place too
     x, y, off, b = run_batch(lengths, seed=11)
+    # chunks of ~32 MiB, at most 32: 32 for the 1.27 GB workload, 1 for the others
+    assert b.diagnostics()["host_chunks"] == (32 if len(lengths) == 20000 else 1)
     assert np.array_equal(_host_run(b, x), y)
     assert np.array_equal(_host_run(b, x, in_place=True), y)
 

@@ -896,7 +896,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
      << bp->long_count[2] << "],\"long_launches\":"
      << ((bp->long_count[0] > 0) + (bp->long_count[1] > 0) + (bp->long_count[2] > 0))
      << ",\"long_grid\":" << bp->grid_long << ",\"long_threads\":" << kLongThreads
-     << ",\"long_smem\":" << bp->smem_long << ",\"cluster_tasks\":" << bp->n_cl
+     << ",\"long_smem\":" << bp->smem_long << ",\"host_chunks\":" << bp->n_chunks
+     << ",\"cluster_tasks\":" << bp->n_cl
      << ",\"kind_lines\":{\"mixed\":" << bp->kind_lines[0] << ",\"rader\":" << bp->kind_lines[1]
      << ",\"bluestein\":" << bp->kind_lines[2] << ",\"cluster_mixed\":" << bp->kind_lines[3]
      << ",\"cluster_bluestein\":" << bp->kind_lines[4] << ",\"two_pass\":" << bp->kind_lines[5]
