@@ -1068,7 +1068,13 @@ static b2f_status run_batch_host(const BatchPlan& bp, cudaStream_t st, const voi
   };
   if (bp.n_cl || bp.n_big) {
     e = cudaMemcpyAsync(dev_in, host_in, bytes, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && run_batch(bp, st, dev_in, dev_out) != B2F_OK) e = cudaErrorLaunchFailure;
+    if (e == cudaSuccess) {
+      const b2f_status r = run_batch(bp, st, dev_in, dev_out);  // restores the device itself
+      if (r != B2F_OK) {
+        if (prev >= 0 && prev != bp.device) cudaSetDevice(prev);
+        return r;  // its message stands
+      }
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, dev_out, bytes, cudaMemcpyDeviceToHost, st);
     return finish();
   }
