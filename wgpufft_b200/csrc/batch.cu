@@ -1,7 +1,7 @@
 // Batched launch of many 1D f32 lines of mixed lengths: host planner and
-// C ABI (b2f_batch_*).  The north-star "batching form": the lines of all the
-// transforms share persistent launches driven by a device work queue; the
-// reference has no counterpart (it records one dispatch chain per plan).
+// C ABI (b2f_batch_*).  The lines of all the transforms share persistent
+// launches driven by device work queues; the reference has no counterpart
+// (it records one dispatch chain per plan).
 #include <algorithm>
 #include <cmath>
 #include <cstring>

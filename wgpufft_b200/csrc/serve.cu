@@ -1,5 +1,6 @@
-// Serving loop (b2f_server_*): the north star's serving form; the crate has
-// no counterpart (its plans only record into a caller's encoder).
+// Serving loop (b2f_server_*): requests of any configuration served with
+// continuous batching; the crate has no counterpart (its plans only record
+// into a caller's encoder).
 //
 // Clients submit transforms of any configuration with their data in host
 // memory.  One scheduler thread owns the device side:
