@@ -90,6 +90,9 @@ struct Server {
   int next_stream = 0;
   // plan cache: key (with the total batch) -> plan
   std::map<std::string, std::unique_ptr<Plan>> plans;
+  // per cached plan, the end of its last execution: a plan's workspace is
+  // shared by its executions, so one on another stream waits for it
+  std::map<const Plan*, cudaEvent_t> plan_done;
   uint64_t plan_bytes = 0;
   // statistics
   std::vector<double> lat;
@@ -109,6 +112,7 @@ struct Server {
       cudaEventSynchronize(g.done);
       cudaEventDestroy(g.done);
     }
+    for (auto& kv : plan_done) cudaEventDestroy(kv.second);
     for (auto s : streams) cudaStreamDestroy(s);
   }
 
@@ -200,7 +204,11 @@ struct Server {
       cudaMemcpyAsync((char*)din + off, r->host_in, r->in_bytes, cudaMemcpyHostToDevice, s);
       off += r->in_bytes;
     }
+    cudaEvent_t& pd = plan_done[plan];
+    if (!pd) cudaEventCreateWithFlags(&pd, cudaEventDisableTiming);
+    else cudaStreamWaitEvent(s, pd, 0);  // after this group's copies in are queued
     st = execute_plan(*plan, s, din, in_total, dout, out_total);
+    if (pd) cudaEventRecord(pd, s);
     off = 0;
     for (SReq* r : members) {
       cudaMemcpyAsync(r->host_out, (char*)dout + off, r->out_bytes, cudaMemcpyDeviceToHost, s);
