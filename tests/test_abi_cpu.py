@@ -202,3 +202,21 @@ def test_tensor_core_knob_routes_and_validates():
     with pytest.raises(w.FftError) as e:
         w.FftConfig.new(64).with_tuning(w.FftTuning().with_tensor_cores(2)).validate()
     assert e.value.kind == "InvalidTuning"
+
+
+def test_batch_argument_checks_before_any_device_call():
+    # b2f_batch_new validates lines on the host (the reference's checked
+    # execution reports the same variants: src/error.rs)
+    cases = [
+        (([], []), {}, "InvalidArgument"),
+        (([16, 0], [0, 16]), {}, "ZeroLength"),
+        (([16, 16], [0, 8]), {}, "InvalidArgument"),          # overlapping lines
+        (([1 << 33], [0]), {}, "LengthTooLarge"),
+        (([16], [(1 << 64) - 8]), {}, "InvalidArgument"),     # beyond the address range
+        (([16], [0]), {"direction": 2}, "InvalidArgument"),
+        (([16], [0]), {"normalization": 7}, "InvalidArgument"),
+    ]
+    for (lengths, offsets), kw, kind in cases:
+        with pytest.raises(w.FftError) as e:
+            w.FftBatch(lengths, offsets, **kw)
+        assert e.value.kind == kind, (lengths, offsets, kw, e.value)

@@ -433,6 +433,8 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     order[i] = i;
     if (lengths[i] == 0) return fail(B2F_ERR_ZERO_LENGTH, "ZeroLength: line " + std::to_string(i));
     if (lengths[i] > 0xFFFFFFFFull) return fail(B2F_ERR_LENGTH_TOO_LARGE, "LengthTooLarge");
+    if (offsets[i] > (UINT64_MAX >> 4) - lengths[i])  // byte sizes must fit 64 bits
+      return fail(B2F_ERR_INVALID_ARGUMENT, "batch line " + std::to_string(i) + " lies beyond the addressable range");
   }
   std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return offsets[a] < offsets[b]; });
   uint64_t extent = 0;
