@@ -22,8 +22,18 @@
  * throws across the ABI.
  *
  * Threading: a plan is immutable after creation and may be executed from
- * several threads on different streams at once, except that the in-place
- * real-transform copy buffer is created on first use under a lock.
+ * several threads on different streams at once.  A plan whose executions
+ * share device memory (a multi-pass route's workspace, the in-place copy
+ * buffer of a real transform, created on first use under a lock) orders
+ * them on the device itself: each execution waits for the previous one's
+ * completion event and records its own, so executions on different streams
+ * run one after the other instead of racing.  Executions recorded into a
+ * CUDA graph (b2f_plan_record, or any stream capture) skip that event pair;
+ * the graph's own order applies, and a graph launched concurrently with an
+ * eager execution of the same plan must be ordered by the caller.  A batch
+ * (b2f_batch_*) keeps its work-queue counters and internal streams per
+ * object: executions of one batch must be ordered by the caller (one
+ * stream, or events).
  */
 #ifndef WGPUFFT_B200_H
 #define WGPUFFT_B200_H
@@ -272,7 +282,9 @@ void b2f_server_reset_stats(b2f_server* server);
  * GPU that loads the library holds the 32 MiB array until the process
  * exits.  The first call on each device looks the array's device address
  * up (cudaGetSymbolAddress, with that device current); make that first
- * call before any stream capture.  All calls share the one array (the last
+ * call before any stream capture.  The address is cached for the life of
+ * the device's primary context: calling cudaDeviceReset on a device
+ * invalidates it, so this entry point must not be used after one.  All calls share the one array (the last
  * call's contents stay in it; every element is rewritten before it is read,
  * so nothing needs clearing), so calls that overlap on the GPU race: issue
  * them on one stream, or order them.  Inputs, outputs, direction and
@@ -280,6 +292,20 @@ void b2f_server_reset_stats(b2f_server* server);
 b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint64_t in_bytes, void* out,
                                   uint64_t out_bytes, uint64_t n, uint64_t batch,
                                   int32_t direction, int32_t normalization);
+
+/* ---------------------------------------------------------- df64 canary */
+
+/* validate_df64_invariants (src/df64_canary.rs:1-8, 101-235): evaluates the
+ * df64 route's error-free transforms (two-sum, quick-two-sum, two-product,
+ * df64 add and multiply, complex add and multiply, an overflow-edge
+ * product, a constant product) on the device on 4 adversarial input cases
+ * and compares each of the 88 f32 words bit for bit with the same
+ * transforms in IEEE single precision on the host.  Returns B2F_OK when all
+ * match; otherwise B2F_ERR_DEVICE with "InvariantMismatch { case, word,
+ * actual, expected }" in b2f_last_error_message.  words (nullable) receives
+ * the 88 device words; *exact_words (nullable) the count that matched
+ * before the first mismatch.  device -1 = the current device. */
+b2f_status b2f_df64_canary(int32_t device, uint32_t* words, uint64_t* exact_words);
 
 /* --------------------------------------------------------------- errors */
 

@@ -153,3 +153,27 @@ def test_batch_execute_host_gaps_inverse_and_clusters(cuda):
     with pytest.raises(w.FftError) as e:
         b.execute_host(hb, hb, db, db)
     assert e.value.kind == "BufferViewTooSmall"
+
+
+@pytest.mark.parametrize("world", [2, 3, 8])
+def test_partitioned_batches_equal_the_whole_batch(cuda, world):
+    # the multi-GPU split (one contiguous run of lines per rank, each run its
+    # own batch over its own buffers) gives every line the same bits as one
+    # batch over all lines; the runs execute one after the other on this GPU
+    import torch
+
+    from wgpufft_b200.replicas import partition_lines
+    lengths = W.mixed_lengths(count=3000, seed=12)
+    x, y_all, off, _ = run_batch(lengths, seed=4)
+    for a, b in partition_lines(lengths, world):
+        if a == b:
+            continue
+        sub = lengths[a:b]
+        lo, hi = int(off[a]), int(off[a] + sub.sum())
+        part = w.FftBatch(sub, W.packed_offsets(sub))
+        dx = torch.from_numpy(x[lo:hi].view(np.float32).copy()).cuda()
+        out = torch.empty_like(dx)
+        part.execute(dx, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().view(np.complex64)
+        assert np.array_equal(got.view(np.uint32), y_all[lo:hi].view(np.uint32)), (a, b)

@@ -163,3 +163,32 @@ def test_computed_twiddles_match_table(cuda):
     b, _, _ = run_c2c(cfg.with_tuning(w.FftTuning().with_twiddle_table(False)), x)
     ref = O.c2c_nd_f64(exact, [4096], batch=4)
     assert O.rel_l2(a, ref) < 2e-6 and O.rel_l2(b, ref) < 2e-6
+
+
+def test_one_multipass_plan_on_two_streams(cuda):
+    # a two-pass (four-step) plan shares its workspace between executions:
+    # executions issued on two streams at once must be ordered by the plan
+    import torch
+    n, batch = 1 << 20, 4
+    cfg = w.FftConfig.new(n).with_batch(batch)
+    plan = w.FftPlan.c2c(cfg)
+    assert plan.workspace_size_bytes() > 0
+    xs = [signal(n * batch, 50 + i) for i in range(2)]
+    devs = [to_device(x, F32) for x in xs]
+    outs = [torch.empty_like(d) for d, _ in devs]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    torch.cuda.synchronize()
+    for _ in range(3):
+        for (d, _), o, s in zip(devs, outs, streams):
+            plan.execute_checked(d, o, stream=s)
+    torch.cuda.synchronize()
+    for (_, exact), o in zip(devs, outs):
+        ref = O.c2c_nd_f64(exact, [n], batch=batch)
+        assert O.rel_l2(from_device(o, F32), ref) <= 2e-6
+
+
+def test_df64_canary_exact_words(cuda):
+    # src/df64_canary.rs: every error-free-transform word of the df64 route
+    # on the device equals the host's IEEE single-precision evaluation
+    rep = w.validate_df64_invariants()
+    assert rep["cases"] == 4 and rep["exact_words"] == 88

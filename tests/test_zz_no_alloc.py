@@ -44,6 +44,7 @@ def test_noalloc_matches_plan_path_twice(cuda, n, batch, direction):
     w.FftPlan.c2c(cfg).execute_checked(dx, ref)
     torch.cuda.synchronize()
     expect = ref.cpu().numpy().view(np.complex64)
+    oracle = O.c2c_nd_f64(x.astype(np.complex128), [n], batch=batch, inverse=direction == 1)
     stream = torch.cuda.current_stream().cuda_stream
     nbytes = dx.numel() * 4
     for call in range(2):
@@ -55,6 +56,8 @@ def test_noalloc_matches_plan_path_twice(cuda, n, batch, direction):
         got = out.cpu().numpy().view(np.complex64)
         err = O.rel_l2(got, expect)
         assert err <= TOL, f"call {call}: rel_l2 {err:.3e} against the plan path"
+        err = O.rel_l2(got, oracle)
+        assert err <= TOL, f"call {call}: rel_l2 {err:.3e} against the FP64 oracle"
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):

@@ -109,6 +109,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_batch_execute_parts": (st, [vp, vp, vp, u64, vp, u64, u32, i32]),
         "b2f_batch_execute_host": (st, [vp, vp, vp, vp, vp, vp, u64]),
         "b2f_c2c_1d_f32_noalloc": (st, [vp, vp, u64, vp, u64, u64, u64, i32, i32]),
+        "b2f_df64_canary": (st, [i32, ctypes.POINTER(u32), ctypes.POINTER(u64)]),
         "b2f_server_new": (st, [pvp, i32, u64, i32, i32]),
         "b2f_server_free": (None, [vp]),
         "b2f_server_submit": (st, [vp, vp, i32, vp, u64, vp, u64, ctypes.POINTER(u64)]),
@@ -679,6 +680,17 @@ def _json_out(fn, *args, cap: int = 1 << 20) -> str:
         st = fn(*args, buf, ctypes.byref(n))
     _check(st)
     return buf.value.decode()
+
+
+def validate_df64_invariants(device: Optional[int] = None) -> dict:
+    """validate_df64_invariants (src/df64_canary.rs): runs the df64 canary
+    on the device; raises FftError (InvariantMismatch detail) when a device
+    word differs from the host's error-free transform."""
+    words = (ctypes.c_uint32 * 88)()
+    exact = ctypes.c_uint64(0)
+    _check(lib().b2f_df64_canary(-1 if device is None else int(device), words,
+                                 ctypes.byref(exact)))
+    return {"cases": 4, "exact_words": int(exact.value), "words": list(words)}
 
 
 def autotune(config: FftConfig, kind: FftTransformKind = FftTransformKind.C2c,

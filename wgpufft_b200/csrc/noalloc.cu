@@ -24,7 +24,11 @@ constexpr uint64_t kNoAllocScratchBytes = 32ull << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of the scratch array per device, looked up once with that
-// device current (the host-side symbol is not a device address).
+// device current (the host-side symbol is not a device address).  The
+// cached address belongs to the device's primary context: it stays valid
+// while that context lives, i.e. until process exit unless the caller
+// resets the device (cudaDeviceReset), which this entry point does not
+// support.
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[128] = {};
 
@@ -99,9 +103,16 @@ extern "C" b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint6
     return fail(B2F_ERR_UNSUPPORTED_LENGTH,
                 "UnsupportedLength { len: " + std::to_string(n) +
                     " } (the allocation-free entry point takes 2,3,5,7,11,13-smooth lengths)");
-  // host-only planning: no device allocation happens for a planning-only plan
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(B2F_ERR_DEVICE, "no current device");
+  // host-only planning (no device allocation) within this device's own
+  // shared-memory limit (a device attribute query allocates nothing)
+  int smem = 0;
+  if (cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      smem <= 0)
+    return fail(B2F_ERR_DEVICE, "could not read the device's shared-memory limit");
   Plan* raw = nullptr;
-  st = create_plan(cfg, B2F_C2C, -2, &raw);
+  st = create_plan(cfg, B2F_C2C, -2, &raw, (size_t)smem);
   if (st) return st;
   std::unique_ptr<Plan> plan(raw);
   if (plan->table_bytes != 0)
@@ -117,8 +128,6 @@ extern "C" b2f_status b2f_c2c_1d_f32_noalloc(void* stream, const void* in, uint6
                 "WorkspaceTooSmall { required: " + std::to_string(need) +
                     ", limit: " + std::to_string(kNoAllocScratchBytes) +
                     " } (n * batch above the static scratch of the allocation-free entry point)");
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return fail(B2F_ERR_DEVICE, "no current device");
   void* scratch = nullptr;
   void* ws[kNumWorkspaces] = {};
   if (need > 0) {

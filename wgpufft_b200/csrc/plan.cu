@@ -998,6 +998,7 @@ Plan::~Plan() {
   for (void* p : ws)
     if (p) cudaFree(p);
   if (inplace_copy) cudaFree(inplace_copy);
+  if (last_done) cudaEventDestroy(last_done);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -1076,7 +1077,8 @@ static void build_diagnostics(Plan& plan) {
   plan.diag_json = os.str();
 }
 
-b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** out) {
+b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** out,
+                       size_t smem_budget) {
   *out = nullptr;
   b2f_status st = validate_config(cfg_in);
   if (st) return st;
@@ -1114,7 +1116,7 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
   plan->route = select_route(cfg);
   Builder b{*plan, dry, 0, {}};
   if (dry) {
-    b.smem_budget = 232448;
+    b.smem_budget = smem_budget ? smem_budget : 232448;
   } else {
     int v = 0;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
@@ -1242,6 +1244,15 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
       }
     }
     b.apply_patches();
+    plan->shared_state = plan->workspace_total() > 0 || !plan->in_place_kernels;
+    for (const Pass& ps : plan->passes)
+      if (ps.kind == Pass::TC_DFT64) plan->shared_state = true;
+    if (plan->shared_state &&
+        cudaEventCreateWithFlags(&plan->last_done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      if (prev >= 0) cudaSetDevice(prev);
+      return fail(B2F_ERR_DEVICE, "plan event creation failed");
+    }
     for (int w = 0; w < kNumWorkspaces; ++w) {
       if (plan->ws_bytes[w] == 0) continue;
       if (cudaMalloc(&plan->ws[w], plan->ws_bytes[w]) != cudaSuccess) {
@@ -1327,6 +1338,36 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
   return B2F_OK;
 }
 
+// Runs f() ordered after the plan's previous execution when the plan holds
+// device state that its executions share (Plan::shared_state): the stream
+// waits for the previous execution's completion event and this execution
+// records a new one.  Executions recorded into a CUDA graph (the stream is
+// capturing) are ordered by the graph itself and skip the events.
+template <class F>
+static b2f_status ordered(const Plan& plan, cudaStream_t st, F&& f) {
+  if (!plan.shared_state || !plan.last_done) return f();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return f();
+  }
+  if (cs != cudaStreamCaptureStatusNone) return f();
+  std::lock_guard<std::mutex> lk(plan.exec_mu);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != plan.device) cudaSetDevice(plan.device);
+  if (plan.last_done_recorded && cudaStreamWaitEvent(st, plan.last_done, 0) != cudaSuccess) {
+    if (prev >= 0 && prev != plan.device) cudaSetDevice(prev);
+    return fail(B2F_ERR_DEVICE, "could not order the execution after the plan's previous one");
+  }
+  const b2f_status s = f();
+  if (cudaEventRecord(plan.last_done, st) == cudaSuccess) plan.last_done_recorded = true;
+  if (prev >= 0 && prev != plan.device) cudaSetDevice(prev);
+  return s;
+}
+
+static b2f_status execute_in_place_impl(const Plan& plan, cudaStream_t st, void* buf);
+
 b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint64_t in_bytes,
                         void* out, uint64_t out_bytes) {
   if (!in || !out) return fail(B2F_ERR_INVALID_ARGUMENT, "null buffer");
@@ -1338,7 +1379,7 @@ b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint6
                                               std::to_string(plan.out_bytes) + ", actual: " + std::to_string(out_bytes) + " }");
   if (in == out && !plan.in_place_kernels)
     return execute_plan_in_place(plan, st, out, std::max(in_bytes, out_bytes));
-  return run_passes(plan, st, in, out);
+  return ordered(plan, st, [&] { return run_passes(plan, st, in, out); });
 }
 
 b2f_status execute_plan_in_place(const Plan& plan, cudaStream_t st, void* buf, uint64_t bytes) {
@@ -1347,6 +1388,10 @@ b2f_status execute_plan_in_place(const Plan& plan, cudaStream_t st, void* buf, u
   if (bytes < need)
     return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall { role: buffer, required: " +
                                               std::to_string(need) + ", actual: " + std::to_string(bytes) + " }");
+  return ordered(plan, st, [&] { return execute_in_place_impl(plan, st, buf); });
+}
+
+static b2f_status execute_in_place_impl(const Plan& plan, cudaStream_t st, void* buf) {
   if (plan.in_place_kernels) return run_passes(plan, st, buf, buf);
   // real transforms: copy the input first, like the crate's in-place copy
   // buffer (src/plan.rs:856-863), created on first use and kept.

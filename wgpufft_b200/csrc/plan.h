@@ -109,6 +109,14 @@ struct Plan {
   bool in_place_kernels = true;  // false: in place copies the input first
   mutable std::mutex copy_mu;
   mutable void* inplace_copy = nullptr;
+  // Executions of a plan with device state shared between them (workspace,
+  // in-place copy buffer, tensor-core error flag) are ordered on the device:
+  // each one waits for the previous one's completion event and records its
+  // own (exec_mu makes the wait/record pair atomic across host threads).
+  bool shared_state = false;
+  mutable std::mutex exec_mu;
+  mutable cudaEvent_t last_done = nullptr;
+  mutable bool last_done_recorded = false;
   std::string diag_json;
   ~Plan();
 };
@@ -119,7 +127,10 @@ std::vector<float> dft64_tc_table();
 cudaError_t launch_dft64_tc(const void* in, void* out, const float* table, uint64_t nlines,
                             float scale, bool inverse, unsigned int* err, unsigned grid,
                             cudaStream_t st);
-b2f_status create_plan(const Config& cfg, int32_t kind, int device, Plan** out);
+// device -2 plans on the host only (no device memory is touched); its
+// shared-memory budget is smem_budget when non-zero, else 232448 bytes.
+b2f_status create_plan(const Config& cfg, int32_t kind, int device, Plan** out,
+                       size_t smem_budget = 0);
 b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint64_t in_bytes,
                         void* out, uint64_t out_bytes);
 b2f_status execute_plan_in_place(const Plan& plan, cudaStream_t st, void* buf, uint64_t bytes);

@@ -1,11 +1,37 @@
-"""Replica plumbing for multi-GPU runs of independent work (batches, mixed
-lines, serving requests): one process per GPU, no data-path collective; the
-only communication is the timing barrier and the max over ranks.  NCCL on
-GPUs, gloo on CPU (the multi-process tests)."""
+"""Multi-GPU plumbing for independent work (batches of lines, serving
+requests): one process per GPU, the lines partitioned across the ranks, no
+data-path collective; the only communication is the timing barrier and the
+max over ranks.  NCCL on GPUs, gloo on CPU (the multi-process tests)."""
 from __future__ import annotations
 
 import os
 from datetime import timedelta
+
+import numpy as np
+
+
+def partition_lines(lengths, world: int):
+    """Splits lines stored back to back into `world` contiguous runs of about
+    equal points (HBM bytes and transform work both grow with the points),
+    so that each rank owns one contiguous range of the buffers.  Returns a
+    list of (first line, end line) per rank; every line belongs to exactly
+    one rank, and a rank may own no line when there are fewer lines than
+    ranks."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    n = len(lengths)
+    if n == 0:
+        return [(0, 0)] * world
+    ends = np.cumsum(lengths)
+    total = int(ends[-1])
+    cuts = [0]
+    for r in range(1, world):
+        # first line whose end passes r/world of the points
+        c = int(np.searchsorted(ends, total * r / world, side="left")) + 1
+        cuts.append(min(max(c, cuts[-1]), n))
+    cuts.append(n)
+    return [(cuts[r], cuts[r + 1]) for r in range(world)]
 
 
 class Replicas:

@@ -74,6 +74,25 @@ def normal_complex(n: int, seed: int) -> np.ndarray:
     return x
 
 
+def uniform_complex(n: int, seed: int) -> np.ndarray:
+    """iid uniform[-1, 1) real and imaginary parts as complex64."""
+    rng = np.random.default_rng(seed)
+    x = np.empty(n, dtype=np.complex64)
+    x.real = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    x.imag = rng.uniform(-1.0, 1.0, n).astype(np.float32)
+    return x
+
+
+def hdr_complex(n: int, seed: int) -> np.ndarray:
+    """High-dynamic-range input: magnitudes log-uniform in [1e-6, 1e6],
+    phases uniform in [0, 2 pi), as complex128 (round to the storage
+    precision before use)."""
+    rng = np.random.default_rng(seed)
+    mag = np.exp(rng.uniform(math.log(1e-6), math.log(1e6), n))
+    ph = rng.uniform(0.0, 2.0 * math.pi, n)
+    return mag * np.exp(1j * ph)
+
+
 def fft_flops(n: int) -> float:
     """The 5 N log2 N convention for one complex transform of length N."""
     return 5.0 * n * math.log2(n) if n > 1 else 0.0
