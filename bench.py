@@ -217,86 +217,115 @@ def cpu_sample_rate(lengths, offsets, x, seconds_target=10.0, threads=0):
         take = min(len(lengths), take * 3)
 
 
-def serving_measurement(local, count=300, rate=2000.0, max_bytes=8 << 20, seed=9):
-    """Open-loop Poisson stream of the serving configuration through the
-    serving loop (resident plans, admission, coalescing, 4 streams) against
-    the plain per-request path (its own plan, copies in, execute, copies out,
-    one request at a time), both with plans created beforehand."""
+def serving_measurement(local, count=300, rates=(1e3, 1e4, 5e4, 1e5, 2e5),
+                        caps=(256 << 20, 8 << 20), seed=9):
+    """The serving configuration: open-loop Poisson request streams (seed 9)
+    of seeded C2C or R2C, forward or inverse requests (1D lengths
+    log-uniform in [64, 2^22], 2D sides from {64..4096}, 3D cubes from
+    {32..256}; batch 1-64; 80/10/10 f32/f64/df64), each request's batch
+    reduced until it holds at most `cap` bytes of input (the stream with
+    256 MiB requests, and one of small requests up to 8 MiB), with their
+    buffers resident in device memory.  At every offered rate: the serving
+    loop (resident plans, 120 GB admission budget, continuous batching:
+    1D complex f32 requests of any length coalesced into one batched line
+    launch, same-configuration requests into one plan execution, 4 streams)
+    against the plain per-request path (one cached plan per configuration,
+    one execute_checked per request as it arrives, on one stream).  Served
+    and plain FFTs/s count the transforms over the span from the first
+    arrival to the last completion; latency is arrival to completion."""
     import threading
 
     import torch
     import wgpufft_b200 as w
     from wgpufft_b200 import workloads as W
 
-    reqs = W.serving_requests(count, seed=seed, max_bytes=max_bytes)
-    rng = np.random.default_rng(seed + 1)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    out = {"requests_per_stream": count, "rates_per_s": list(rates), "buffers": "device",
+           "streams": {}}
+    for cap in caps:
+        reqs = W.serving_requests(count, seed=seed, max_bytes=cap)
 
-    def cfg_of(q):
-        c = w.FftConfig.new_nd(q["shape"]).with_batch(q["batch"]).with_precision(q["precision"])
-        return c.with_direction(w.FftDirection.Inverse if q["inverse"] else w.FftDirection.Forward)
+        def cfg_of(q):
+            c = w.FftConfig.new_nd(q["shape"]).with_batch(q["batch"]).with_precision(q["precision"])
+            return c.with_direction(w.FftDirection.Inverse if q["inverse"] else w.FftDirection.Forward)
 
-    cfgs = [cfg_of(q) for q in reqs]
-    kinds = [w.FftTransformKind(q["kind"]) for q in reqs]
-    plans = [{0: w.FftPlan.c2c, 1: w.FftPlan.r2c, 2: w.FftPlan.c2r}[int(k)](c, device=local)
-             for c, k in zip(cfgs, kinds)]
-    ins, outs = [], []
-    for p in plans:
-        ib, ob = p.required_input_buffer_size_bytes(), p.required_output_buffer_size_bytes()
-        ins.append(torch.zeros(ib // 4, dtype=torch.float32).pin_memory())
-        outs.append(torch.zeros(ob // 4, dtype=torch.float32).pin_memory())
-    transforms = sum(q["batch"] for q in reqs)
-    # plain per-request path
-    stream = torch.cuda.current_stream()
-    din = torch.empty(max(t.numel() for t in ins), dtype=torch.float32, device="cuda")
-    dout = torch.empty(max(t.numel() for t in outs), dtype=torch.float32, device="cuda")
-    for p, hi, ho in zip(plans[:8], ins, outs):  # warm-up
-        p.execute_checked((din.data_ptr(), din.numel() * 4), (dout.data_ptr(), dout.numel() * 4))
-    torch.cuda.synchronize()
-    lat_plain = []
-    t0 = time.perf_counter()
-    for i, (p, hi, ho) in enumerate(zip(plans, ins, outs)):
-        while time.perf_counter() - t0 < arrivals[i]:
-            pass
-        din[:hi.numel()].copy_(hi, non_blocking=True)
-        p.execute_checked((din.data_ptr(), din.numel() * 4), (dout.data_ptr(), dout.numel() * 4))
-        ho.copy_(dout[:ho.numel()], non_blocking=True)
+        cfgs = [cfg_of(q) for q in reqs]
+        kinds = [w.FftTransformKind(q["kind"]) for q in reqs]
+        mk = {0: w.FftPlan.c2c, 1: w.FftPlan.r2c, 2: w.FftPlan.c2r}
+        plans, by_key = [], {}
+        for c, k in zip(cfgs, kinds):
+            key = (int(k), tuple(c.shape()), c.batch(), int(c.precision()), int(c.direction()))
+            if key not in by_key:
+                by_key[key] = mk[int(k)](c, device=local)
+            plans.append(by_key[key])
+        ins, outs = [], []
+        for p in plans:
+            ins.append(torch.randn(p.required_input_buffer_size_bytes() // 4, device="cuda"))
+            outs.append(torch.empty(p.required_output_buffer_size_bytes() // 4, device="cuda"))
+        transforms = sum(q["batch"] for q in reqs)
+        in_bytes = sum(t.numel() * 4 for t in ins)
+        stream = torch.cuda.current_stream()
+        # warm-up: every plan once; the serving loop's resident plans and line lengths
+        for p, a, b in zip(plans, ins, outs):
+            p.execute_checked(a, b)
         torch.cuda.synchronize()
-        lat_plain.append(time.perf_counter() - t0 - arrivals[i])
-    plain_span = time.perf_counter() - t0 - arrivals[0]
-    del plans
-    # served path (plans become resident during a first unmeasured pass)
-    srv = w.FftServer(device=local, streams=4)
-    warm = [srv.submit(c, k, hi, ho) for c, k, hi, ho in zip(cfgs, kinds, ins, outs)]
-    for r in warm:
-        srv.wait(r, 600.0)
-    srv.reset_stats()
-    ids = [None] * len(reqs)
+        srv = w.FftServer(device=local, streams=4)
+        for r in [srv.submit_device(c, k, a, b) for c, k, a, b in zip(cfgs, kinds, ins, outs)]:
+            srv.wait(r, 600.0)
+        per_rate = []
+        for rate in rates:
+            rng = np.random.default_rng(seed + 1)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+            # plain per-request path: completion events timed on the device
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(reqs) + 1)]
+            t_sub = []
+            torch.cuda.synchronize()
+            evs[0].record(stream)
+            t0 = time.perf_counter()
+            for i, (p, a, b) in enumerate(zip(plans, ins, outs)):
+                while time.perf_counter() - t0 < arrivals[i]:
+                    pass
+                t_sub.append(time.perf_counter() - t0)
+                p.execute_checked(a, b)
+                evs[i + 1].record(stream)
+            torch.cuda.synchronize()
+            done = [evs[0].elapsed_time(e) / 1e3 for e in evs[1:]]
+            lat_plain = sorted(max(d - a, d - t) for d, a, t in zip(done, arrivals, t_sub))
+            span_plain = max(done) - arrivals[0]
+            # served
+            srv.reset_stats()
+            ids = [None] * len(reqs)
 
-    def feeder():
-        t1 = time.perf_counter()
-        for i in range(len(reqs)):
-            while time.perf_counter() - t1 < arrivals[i]:
-                pass
-            ids[i] = srv.submit(cfgs[i], kinds[i], ins[i], outs[i])
+            def feeder():
+                t1 = time.perf_counter()
+                for i in range(len(reqs)):
+                    while time.perf_counter() - t1 < arrivals[i]:
+                        pass
+                    ids[i] = srv.submit_device(cfgs[i], kinds[i], ins[i], outs[i])
 
-    th = threading.Thread(target=feeder)
-    th.start()
-    th.join()
-    srv.drain(600.0)
-    st = srv.stats()
-    for r in ids:
-        srv.wait(r, 60.0)
-    srv.close()
-    lp = sorted(lat_plain)
-    plain = {"ffts_per_s": transforms / plain_span, "requests_per_s": len(reqs) / plain_span,
-             "p50_ms": lp[len(lp) // 2] * 1e3, "p99_ms": lp[int(len(lp) * 0.99)] * 1e3}
-    served = {"ffts_per_s": st["ffts_per_s"], "requests_per_s": st["requests_per_s"],
-              "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "groups": st["groups"],
-              "coalesced_requests": st["coalesced_requests"]}
-    return {"requests": len(reqs), "offered_rate_per_s": rate, "transforms": transforms,
-            "max_request_bytes": max_bytes, "served": served, "plain_per_request": plain,
-            "served_vs_plain_ffts": served["ffts_per_s"] / max(plain["ffts_per_s"], 1e-9)}
+            th = threading.Thread(target=feeder)
+            th.start()
+            th.join()
+            srv.drain(600.0)
+            st = srv.stats()
+            for r in ids:
+                srv.wait(r, 60.0)
+            plain = {"ffts_per_s": transforms / span_plain, "p50_ms": lat_plain[len(lat_plain) // 2] * 1e3,
+                     "p99_ms": lat_plain[int(len(lat_plain) * 0.99)] * 1e3}
+            served = {"ffts_per_s": st["ffts_per_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                      "groups": st["groups"], "line_groups": st["line_groups"],
+                      "coalesced_requests": st["coalesced_requests"]}
+            per_rate.append({"offered_rate_per_s": rate, "served": served,
+                             "plain_per_request": plain,
+                             "served_vs_plain_ffts": served["ffts_per_s"] / max(plain["ffts_per_s"], 1e-9)})
+        stats = srv.stats()
+        srv.close()
+        out["streams"][f"max_{cap >> 20}MiB"] = {
+            "transforms": transforms, "input_bytes": in_bytes, "distinct_configs": len(by_key),
+            "resident_plans": stats["resident_plans"], "per_rate": per_rate,
+            "served_vs_plain_at_saturation": per_rate[-1]["served_vs_plain_ffts"]}
+        del plans, by_key, ins, outs
+        torch.cuda.empty_cache()
+    return out
 
 
 def config_measurements(local, hbm_peak):
@@ -395,7 +424,8 @@ def config_measurements(local, hbm_peak):
         shape = cfg.shape()
         nd = len(shape)
         axes = tuple(range(1, nd + 1))  # numpy axes of [batch, ..., axis1, axis0]
-        arr = exact.reshape([cfg.batch()] + shape[::-1])
+        stored = shape if kind != C2R else [shape[0] // 2 + 1] + shape[1:]
+        arr = exact.reshape([cfg.batch()] + stored[::-1])
         inv = cfg.direction() == w.FftDirection.Inverse
         norm = {0: "backward", 1: "forward", 2: "backward", 3: "ortho"}[int(cfg.normalization())]
         if int(cfg.normalization()) == 0:

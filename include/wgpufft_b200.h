@@ -72,6 +72,11 @@ typedef int32_t b2f_status;
 #define B2F_ERR_SNAPSHOT_SCHEMA 19         /* PipelineCacheSnapshotError::SchemaMismatch */
 #define B2F_ERR_SNAPSHOT_VERSION 20        /* PipelineCacheSnapshotError::VersionMismatch */
 #define B2F_ERR_SNAPSHOT_INTEGRITY 21      /* PipelineCacheSnapshotError::Integrity */
+/* Logical views (src/error.rs:65-77). */
+#define B2F_ERR_LAYOUT_ZERO_STRIDE 22            /* FftError::BufferLayoutZeroStride */
+#define B2F_ERR_LAYOUT_BATCH_STRIDE_TOO_SMALL 23 /* FftError::BufferLayoutBatchStrideTooSmall */
+#define B2F_ERR_LAYOUT_OUT_OF_BOUNDS 24          /* FftError::BufferLayoutOutOfBounds */
+#define B2F_ERR_LAYOUT_TOO_LARGE 25              /* FftError::BufferLayoutTooLarge */
 
 /* FftDirection (src/config.rs:43-57). */
 #define B2F_FORWARD 0
@@ -169,6 +174,40 @@ b2f_status b2f_plan_execute_in_place(const b2f_plan* plan, void* stream, void* b
  * buffer requirements and requested/effective tuning.  On entry *len is the
  * capacity of buf; on return it is the length needed (without the NUL). */
 b2f_status b2f_plan_diagnostics_json(const b2f_plan* plan, char* buf, uint64_t* len);
+/* No counterpart in the crate (wgpu reports device loss through its own
+ * callbacks): waits for the plan's device work (synchronising its device)
+ * and reports whether a bounded device-side wait of its kernels gave up
+ * (the tensor-core layer's waits for its matrix products), clearing the
+ * flag.  B2F_OK when none did, else B2F_ERR_DEVICE with the detail. */
+b2f_status b2f_plan_device_status(const b2f_plan* plan);
+
+/* FftLogicalLayout (src/runtime/logical_io.rs:34-38, 90-110): logical
+ * element i of batch b sits at element element_offset + b * batch_stride +
+ * i * element_stride of the buffer, counted in the endpoint's elements (a
+ * complex value of the plan's precision; a real value on the real side of
+ * an R2C/C2R plan).  element_stride 0 is rejected (BufferLayoutZeroStride);
+ * batch_stride 0 means None, i.e. the per-batch span
+ * element_stride * (elements - 1) + 1, and a smaller nonzero value is
+ * rejected (BufferLayoutBatchStrideTooSmall). */
+typedef struct b2f_logical_layout {
+  uint64_t element_offset;
+  uint64_t element_stride;
+  uint64_t batch_stride;
+} b2f_logical_layout;
+
+/* FftPlan::execute_logical_views / execute_views (src/plan.rs:580-806):
+ * the plan between two caller views.  A NULL layout is the contiguous view
+ * (offset 0, stride 1).  A wgpu BufferView (buffer, offset, size) is the
+ * pointer advanced by the offset with its size: execute_views needs no
+ * separate entry point.  Contiguous and offset-only layouts run on the
+ * caller's memory directly; strided layouts gather the input into, and/or
+ * scatter the output from, staging buffers the plan allocates on first use
+ * and keeps.  Sizes: the view must hold offset + (batch - 1) * batch_stride
+ * + span elements (BufferLayoutOutOfBounds otherwise). */
+b2f_status b2f_plan_execute_logical_views(const b2f_plan* plan, void* stream, const void* in,
+                                          uint64_t in_bytes, const b2f_logical_layout* in_layout,
+                                          void* out, uint64_t out_bytes,
+                                          const b2f_logical_layout* out_layout);
 
 /* ---------------------------------------------------------- FftRecorder */
 
@@ -243,11 +282,18 @@ b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_
 
 /* Serving loop (no counterpart in the crate): a scheduler thread that keeps
  * plans, tables and workspaces resident, admits requests by an HBM budget,
- * coalesces queued requests of the same configuration into one batched
- * execution (continuous batching: arrivals join the next group while
- * earlier ones run), and overlaps groups on `nstreams` streams.  Requests
- * carry host buffers (pinned memory lets the copies overlap); results are
- * written back to host_out.  hbm_budget_bytes 0 = 120 GB. */
+ * and batches continuously (arrivals join the next group while earlier
+ * ones run), overlapping groups on `nstreams` streams.  1D complex f32
+ * requests of one direction and normalization are coalesced whatever their
+ * lengths into one batched launch of the mixed-length line kernels; other
+ * requests of the same configuration are coalesced into one execution of a
+ * resident plan (plans keyed by configuration and a power-of-two batch
+ * bucket, evicted least recently used when the budget needs the room).
+ * Requests carry host buffers (pinned memory lets the copies overlap;
+ * results are written back to host_out) or device buffers
+ * (b2f_server_submit_device).  When a group fails, no copy touching a
+ * request's memory is pending by the time its wait returns the error.
+ * hbm_budget_bytes 0 = 120 GB. */
 typedef struct b2f_server b2f_server;
 b2f_status b2f_server_new(b2f_server** out, int32_t device, uint64_t hbm_budget_bytes,
                           int32_t nstreams, int32_t coalesce);
@@ -256,6 +302,13 @@ void b2f_server_free(b2f_server* server);
 b2f_status b2f_server_submit(b2f_server* server, const b2f_config* cfg, int32_t kind,
                              const void* host_in, uint64_t in_bytes, void* host_out,
                              uint64_t out_bytes, uint64_t* request_id);
+/* b2f_server_submit with the request's buffers in device memory of the
+ * server's device: the transform reads and writes them where they lie (no
+ * host copies).  1D complex f32 requests need 8-byte aligned buffers to
+ * join a batched line launch; others run alone. */
+b2f_status b2f_server_submit_device(b2f_server* server, const b2f_config* cfg, int32_t kind,
+                                    const void* dev_in, uint64_t in_bytes, void* dev_out,
+                                    uint64_t out_bytes, uint64_t* request_id);
 /* Blocks until the request completed (or timeout_s passed; 0 = 1 hour). */
 b2f_status b2f_server_wait(b2f_server* server, uint64_t request_id, double timeout_s);
 /* Blocks until nothing is queued or in flight. */

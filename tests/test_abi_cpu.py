@@ -220,3 +220,28 @@ def test_batch_argument_checks_before_any_device_call():
         with pytest.raises(w.FftError) as e:
             w.FftBatch(lengths, offsets, **kw)
         assert e.value.kind == kind, (lengths, offsets, kw, e.value)
+
+
+def test_layout_status_strings():
+    # src/error.rs:65-77
+    L = w.lib()
+    assert [L.b2f_status_string(c) for c in (22, 23, 24, 25)] == [
+        b"BufferLayoutZeroStride", b"BufferLayoutBatchStrideTooSmall",
+        b"BufferLayoutOutOfBounds", b"BufferLayoutTooLarge"]
+
+
+def test_small_volume_eligibility():
+    # src/runtime/small_volume.rs:223-272: f32, rank >= 2, every axis, at most
+    # 4096 points, smooth axes, no forced axes, fuse_small_volumes on
+    def labels(cfg):
+        return [s["label"] for s in plan_only(cfg).diagnostics()["stages"]]
+    for shape in ([8, 8, 8], [64, 64], [16, 16, 16], [3, 5, 7], [2, 2048]):
+        assert labels(w.FftConfig.new_nd(shape).with_batch(3)) == ["small-volume-stage"], shape
+    assert "small-volume-stage" not in labels(w.FftConfig.new_nd([64, 128]))       # 8192 points
+    assert "small-volume-stage" not in labels(w.FftConfig.new_nd([8, 29, 4]))       # prime axis
+    assert "small-volume-stage" not in labels(w.FftConfig.new(4096))               # rank 1
+    assert "small-volume-stage" not in labels(w.FftConfig.new_nd([8, 8]).with_axes([1]))
+    assert "small-volume-stage" not in labels(
+        w.FftConfig.new_nd([8, 8]).with_precision(w.FftPrecision.F64))
+    assert "small-volume-stage" not in labels(
+        w.FftConfig.new_nd([8, 8]).with_tuning(w.FftTuning().with_fuse_small_volumes(False)))

@@ -192,3 +192,28 @@ def test_df64_canary_exact_words(cuda):
     # on the device equals the host's IEEE single-precision evaluation
     rep = w.validate_df64_invariants()
     assert rep["cases"] == 4 and rep["exact_words"] == 88
+
+
+@pytest.mark.parametrize("shape,batch", [([8, 8, 8], 1), ([16, 16, 16], 2), ([64, 64], 3),
+                                         ([12, 25, 2], 2), ([3, 5, 7], 5), ([2, 2048], 1),
+                                         ([13, 11, 9], 4)])
+def test_small_volume_route(cuda, shape, batch):
+    # src/runtime/small_volume.rs: every axis of a <= 4096-point f32 volume
+    # in one kernel; same results as the oracle, forward and inverse, every
+    # normalisation, in place
+    cfg = w.FftConfig.new_nd(shape).with_batch(batch)
+    labels = [s["label"] for s in w.FftPlan.c2c(cfg).diagnostics()["stages"]]
+    if np.prod(shape) <= 4096 and min(shape) > 1:
+        assert labels == ["small-volume-stage"], labels
+    check_c2c(cfg, seed=60)
+    check_c2c(cfg.with_direction(INV), seed=61)
+    for norm in w.Normalization:
+        check_c2c(cfg.with_normalization(norm).with_direction(INV), seed=62)
+    check_c2c(cfg, seed=63, in_place=True)
+
+
+def test_small_volume_knob_off_uses_axis_passes(cuda):
+    cfg = w.FftConfig.new_nd([16, 16]).with_tuning(w.FftTuning().with_fuse_small_volumes(False))
+    labels = [s["label"] for s in w.FftPlan.c2c(cfg).diagnostics()["stages"]]
+    assert "small-volume-stage" not in labels and len(labels) == 2
+    check_c2c(cfg, seed=64)

@@ -127,3 +127,93 @@ def test_admission_refuses_oversized_request(cuda):
         srv.wait(rid, 30.0)
     assert e.value.kind == "GpuPlanResourceAllocationFailed"
     srv.close()
+
+
+def _line_requests(rng, lengths, batches, inverse=False):
+    cfgs, ins, outs = [], [], []
+    for n, b in zip(lengths, batches):
+        cfg = w.FftConfig.new(int(n)).with_batch(int(b))
+        if inverse:
+            cfg = cfg.with_direction(w.FftDirection.Inverse)
+        hin, hout = host_arrays(cfg, w.FftTransformKind.C2c, rng)
+        cfgs.append(cfg)
+        ins.append(hin)
+        outs.append(hout)
+    return cfgs, ins, outs
+
+
+def test_lines_of_different_lengths_share_one_launch(cuda):
+    # 1D complex f32 requests of any length are coalesced into one batched
+    # launch of the mixed-length line kernels: short lines on the CTA queue,
+    # Rader and Bluestein lengths, long smooth and long Bluestein lines; each
+    # result matches the FP64 oracle and the same request served alone
+    rng = np.random.default_rng(7)
+    lengths = [16, 100, 127, 1009, 1024, 3003, 4099, 20000, 65536, 60013, 17, 243]
+    batches = [5, 3, 2, 4, 8, 2, 1, 1, 1, 1, 64, 7]
+    cfgs, ins, outs = _line_requests(rng, lengths, batches)
+    srv = w.FftServer(streams=2)
+    ids = [srv.submit(c, w.FftTransformKind.C2c, i, o) for c, i, o in zip(cfgs, ins, outs)]
+    srv.drain(120.0)
+    st = srv.stats()
+    for i in ids:
+        srv.wait(i, 10.0)
+    assert st["line_groups"] >= 1 and st["coalesced_requests"] > 0, st
+    assert st["groups"] < len(ids), st
+    for cfg, hin, hout in zip(cfgs, ins, outs):
+        n = cfg.shape()[0]
+        x = hin.numpy().view(np.complex64).astype(np.complex128)
+        ref = O.c2c_nd_f64(x, [n], batch=cfg.batch())
+        got = hout.numpy().view(np.complex64).astype(np.complex128)
+        assert O.rel_l2(got, ref) <= 2e-6, n
+    srv.close()
+    # alone: each request through a fresh server of its own
+    for cfg, hin, hout in zip(cfgs, ins, outs):
+        solo = w.FftServer(streams=1)
+        _, out2 = host_arrays(cfg, w.FftTransformKind.C2c, rng)
+        solo.wait(solo.submit(cfg, w.FftTransformKind.C2c, hin, out2), 60.0)
+        a = hout.numpy().view(np.complex64).astype(np.complex128)
+        b = out2.numpy().view(np.complex64).astype(np.complex128)
+        assert O.rel_l2(a, b) <= 2e-6
+        solo.close()
+
+
+def test_device_buffer_requests(cuda):
+    import torch
+    rng = np.random.default_rng(8)
+    srv = w.FftServer(streams=3)
+    items = [(w.FftConfig.new(4096).with_batch(3), w.FftTransformKind.C2c),
+             (w.FftConfig.new(777).with_batch(2), w.FftTransformKind.C2c),
+             (w.FftConfig.inverse(30011), w.FftTransformKind.C2c),
+             (w.FftConfig.new_nd([64, 48]).with_batch(2), w.FftTransformKind.C2c),
+             (w.FftConfig.new_nd([32, 32, 32]), w.FftTransformKind.R2c),
+             (w.FftConfig.new(1000).with_precision(w.FftPrecision.F64), w.FftTransformKind.C2c)]
+    reqs = []
+    for cfg, kind in items * 2:
+        hin, hout = host_arrays(cfg, kind, rng)
+        din, dout = hin.cuda(), torch.zeros_like(hout).cuda()
+        reqs.append((cfg, kind, hin, din, dout, srv.submit_device(cfg, kind, din, dout)))
+    for cfg, kind, hin, din, dout, rid in reqs:
+        srv.wait(rid, 60.0)
+        ref = alone(cfg, kind, hin)
+        prec = cfg.precision()
+        got = dout.cpu().numpy()
+        assert O.rel_l2(as_complex(got, prec), as_complex(ref, prec)) <= TOL[prec], cfg.shape()
+    st = srv.stats()
+    assert st["failed"] == 0 and st["line_groups"] >= 1, st
+    srv.close()
+
+
+def test_plan_buckets_bound_the_resident_plans(cuda):
+    # one configuration at batches 1..12: the executions run on plans of
+    # power-of-two batches, so at most four plans (1, 2, 4, 8) become resident
+    rng = np.random.default_rng(9)
+    srv = w.FftServer(streams=1, coalesce=False)
+    for b in range(1, 13):
+        cfg = w.FftConfig.new_nd([32, 24]).with_batch(b)
+        hin, hout = host_arrays(cfg, w.FftTransformKind.C2c, rng)
+        srv.wait(srv.submit(cfg, w.FftTransformKind.C2c, hin, hout), 30.0)
+        x = hin.numpy().view(np.complex64).astype(np.complex128)
+        ref = O.c2c_nd_f64(x, [32, 24], batch=b)
+        assert O.rel_l2(hout.numpy().view(np.complex64), ref) <= 2e-6
+    assert srv.stats()["resident_plans"] <= 4
+    srv.close()

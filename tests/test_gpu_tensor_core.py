@@ -44,3 +44,15 @@ def test_other_shapes_ignore_the_knob(cuda):
     plan = w.FftPlan.c2c(_tc(w.FftConfig.new(128).with_batch(8)))
     assert all(s["kind"] != "tensor-core-dft" for s in plan.diagnostics()["stages"])
     check_c2c(_tc(w.FftConfig.new(128).with_batch(8)), seed=7)
+
+
+def test_no_bounded_wait_gave_up(cuda):
+    # every wait of the layer for its matrix products completes: the plan's
+    # device status (the kernel's error flag, read on the host) stays clear
+    import torch
+    plan = w.FftPlan.c2c(_tc(w.FftConfig.new(64).with_batch(50000)))
+    a = torch.randn(64 * 50000 * 2, device="cuda")
+    o = torch.empty_like(a)
+    for _ in range(3):
+        plan.execute_checked(a, o)
+    plan.device_status()

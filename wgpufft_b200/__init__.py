@@ -28,6 +28,7 @@ from typing import Iterable, Optional, Sequence, Tuple, Union
 __all__ = [
     "FftDirection", "Normalization", "FftPrecision", "FftTransformKind", "FftTuning",
     "FftConfig", "FftPlan", "FftRecorder", "FftBatch", "FftServer", "FftError", "lib",
+    "FftLogicalLayout", "validate_df64_invariants",
     "library_path",
 ]
 
@@ -92,7 +93,10 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_plan_supports_in_place": (i32, [vp]),
         "b2f_plan_execute_checked": (st, [vp, vp, vp, u64, vp, u64]),
         "b2f_plan_execute_in_place": (st, [vp, vp, vp, u64]),
+        "b2f_plan_execute_logical_views": (st, [vp, vp, vp, u64, ctypes.POINTER(_Layout), vp, u64,
+                                                ctypes.POINTER(_Layout)]),
         "b2f_plan_diagnostics_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
+        "b2f_plan_device_status": (st, [vp]),
         "b2f_recorder_begin": (st, [pvp, vp]),
         "b2f_plan_record": (st, [vp, vp, vp, u64, vp, u64]),
         "b2f_plan_record_in_place": (st, [vp, vp, vp, u64]),
@@ -113,6 +117,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_server_new": (st, [pvp, i32, u64, i32, i32]),
         "b2f_server_free": (None, [vp]),
         "b2f_server_submit": (st, [vp, vp, i32, vp, u64, vp, u64, ctypes.POINTER(u64)]),
+        "b2f_server_submit_device": (st, [vp, vp, i32, vp, u64, vp, u64, ctypes.POINTER(u64)]),
         "b2f_server_wait": (st, [vp, u64, ctypes.c_double]),
         "b2f_server_drain": (st, [vp, ctypes.c_double]),
         "b2f_server_stats_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
@@ -411,6 +416,33 @@ def _stream(s) -> int:
     return int(s.cuda_stream)
 
 
+class _Layout(ctypes.Structure):
+    _fields_ = [("element_offset", ctypes.c_uint64), ("element_stride", ctypes.c_uint64),
+                ("batch_stride", ctypes.c_uint64)]
+
+
+class FftLogicalLayout:
+    """FftLogicalLayout (src/runtime/logical_io.rs:34-110): logical element i
+    of batch b at element element_offset + b * batch_stride + i *
+    element_stride of a view (batch_stride None = the per-batch span)."""
+
+    def __init__(self, element_offset: int = 0, element_stride: int = 1,
+                 batch_stride: Optional[int] = None):
+        self.element_offset = int(element_offset)
+        self.element_stride = int(element_stride)
+        self.batch_stride = None if batch_stride is None else int(batch_stride)
+
+    @classmethod
+    def contiguous(cls) -> "FftLogicalLayout":
+        return cls()
+
+    def with_batch_stride(self, batch_stride: int) -> "FftLogicalLayout":
+        return FftLogicalLayout(self.element_offset, self.element_stride, batch_stride)
+
+    def _c(self) -> _Layout:
+        return _Layout(self.element_offset, self.element_stride, self.batch_stride or 0)
+
+
 class FftPlan:
     """FftPlan (src/plan.rs:32-1300)."""
 
@@ -499,6 +531,11 @@ class FftPlan:
             self._diag = json.loads(buf.value.decode())
         return self._diag
 
+    def device_status(self) -> None:
+        """Synchronises the plan's device and raises FftError when a bounded
+        device-side wait of its kernels gave up (b2f_plan_device_status)."""
+        _check(lib().b2f_plan_device_status(self._ptr))
+
     def route(self) -> str:
         return self.diagnostics()["route"]
 
@@ -526,6 +563,18 @@ class FftPlan:
     def execute_in_place(self, buffer: Buffer, stream=None) -> None:
         bp, bb = _buf(buffer)
         _check(lib().b2f_plan_execute_in_place(self._ptr, _stream(stream), bp, bb))
+
+    def execute_logical_views(self, input: Buffer, input_layout: Optional[FftLogicalLayout],
+                              output: Buffer, output_layout: Optional[FftLogicalLayout],
+                              stream=None) -> None:
+        """FftPlan::execute_logical_views (src/plan.rs:580-806); None is the
+        contiguous layout."""
+        ip, ib = _buf(input)
+        op, ob = _buf(output)
+        li = ctypes.byref(input_layout._c()) if input_layout is not None else None
+        lo = ctypes.byref(output_layout._c()) if output_layout is not None else None
+        _check(lib().b2f_plan_execute_logical_views(self._ptr, _stream(stream), ip, ib, li, op,
+                                                    ob, lo))
 
     def record(self, recorder: "FftRecorder", input: Buffer, output: Buffer) -> None:
         ip, ib = _buf(input)
@@ -631,6 +680,18 @@ class FftServer:
             _check(lib().b2f_server_submit(self._ptr, h.ptr, int(kind), ip, ib, op, ob,
                                            ctypes.byref(rid)))
         self._keep[rid.value] = (host_in, host_out)
+        return rid.value
+
+    def submit_device(self, config: FftConfig, kind: FftTransformKind, dev_in, dev_out) -> int:
+        """b2f_server_submit_device: dev_in/dev_out are CUDA tensors or
+        (address, nbytes) pairs (kept alive until the request is waited for)."""
+        ip, ib = _buf(dev_in)
+        op, ob = _buf(dev_out)
+        rid = ctypes.c_uint64()
+        with config._handle() as h:
+            _check(lib().b2f_server_submit_device(self._ptr, h.ptr, int(kind), ip, ib, op, ob,
+                                                  ctypes.byref(rid)))
+        self._keep[rid.value] = (dev_in, dev_out)
         return rid.value
 
     def wait(self, request_id: int, timeout_s: float = 0.0) -> None:

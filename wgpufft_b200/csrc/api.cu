@@ -6,9 +6,6 @@
 
 using namespace b2f;
 
-struct b2f_plan {
-  Plan* plan;
-};
 struct b2f_recorder {
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -216,6 +213,32 @@ b2f_status b2f_plan_execute_in_place(const b2f_plan* plan, void* stream, void* b
   return execute_plan_in_place(*plan->plan, (cudaStream_t)stream, buffer, bytes);
 }
 
+b2f_status b2f_plan_device_status(const b2f_plan* plan) {
+  REQUIRE(plan, "null plan");
+  const Plan& p = *plan->plan;
+  if (p.device < 0) return B2F_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != p.device) cudaSetDevice(p.device);
+  uint32_t flags = 0;
+  cudaError_t e = cudaSuccess;
+  for (const Pass& ps : p.passes) {
+    if (ps.kind != Pass::TC_DFT64) continue;
+    uint32_t v = 0;
+    void* d = p.device_allocs[ps.tc_err];
+    e = cudaMemcpy(&v, d, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v) e = cudaMemset(d, 0, sizeof(v));
+    if (e != cudaSuccess) break;
+    flags |= v;
+  }
+  if (prev >= 0 && prev != p.device) cudaSetDevice(prev);
+  if (e != cudaSuccess) return fail(B2F_ERR_DEVICE, std::string("device status read failed: ") + cudaGetErrorString(e));
+  if (flags)
+    return fail(B2F_ERR_DEVICE, std::string("tensor-core layer: a bounded wait for its matrix products timed out") +
+                                    ((flags & 2) ? " (tensor memory freed with a product still pending)" : ""));
+  return B2F_OK;
+}
+
 b2f_status b2f_plan_diagnostics_json(const b2f_plan* plan, char* buf, uint64_t* len) {
   REQUIRE(plan && len, "null argument");
   const std::string& j = plan->plan->diag_json;
@@ -324,6 +347,10 @@ const char* b2f_status_string(b2f_status s) {
     case B2F_ERR_SNAPSHOT_SCHEMA: return "SnapshotSchemaMismatch";
     case B2F_ERR_SNAPSHOT_VERSION: return "SnapshotVersionMismatch";
     case B2F_ERR_SNAPSHOT_INTEGRITY: return "SnapshotIntegrity";
+    case B2F_ERR_LAYOUT_ZERO_STRIDE: return "BufferLayoutZeroStride";
+    case B2F_ERR_LAYOUT_BATCH_STRIDE_TOO_SMALL: return "BufferLayoutBatchStrideTooSmall";
+    case B2F_ERR_LAYOUT_OUT_OF_BOUNDS: return "BufferLayoutOutOfBounds";
+    case B2F_ERR_LAYOUT_TOO_LARGE: return "BufferLayoutTooLarge";
     default: return "Unknown";
   }
 }

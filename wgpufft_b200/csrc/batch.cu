@@ -7,12 +7,14 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <thread>
 
 #include "batch.cuh"
 #include "longpass.cuh"
 #include "hostfft.h"
+#include "linebatch.h"
 #include "plan.h"
 
 namespace b2f {
@@ -415,7 +417,15 @@ static bool classify(uint64_t N, int32_t direction, int32_t normalization, size_
 // soon as static plus dynamic shared memory exceeds 48 KB).
 template <class K>
 static cudaError_t set_smem(K kernel, size_t smem) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the attribute is per kernel for the whole process, shared by every
+  // batch and line registry: always raise it to the device's limit, so no
+  // later, smaller setting can make another object's launch fail
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    optin = (int)smem;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              std::max<int>(optin, (int)smem));
 }
 
 static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets, uint64_t nlines,
@@ -619,16 +629,16 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
         bp->lines_long += 1;
         const uint32_t ch = chunk_of[line];
         for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
-          long_tasks[0].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
+          long_tasks[0].push_back(LongTask{lbase, lscr, (uint32_t)li, g0, lbase});
           long_task_chunk[0].push_back(ch);
         }
         for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr) {
-          long_tasks[1].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
+          long_tasks[1].push_back(LongTask{lbase, lscr, (uint32_t)li, g0, lbase});
           long_task_chunk[1].push_back(ch);
         }
         if (g.blue)
           for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc) {
-            long_tasks[2].push_back(LongTask{lbase, lscr, (uint32_t)li, g0});
+            long_tasks[2].push_back(LongTask{lbase, lscr, (uint32_t)li, g0, lbase});
             long_task_chunk[2].push_back(ch);
           }
       }
@@ -1104,6 +1114,373 @@ static b2f_status run_batch_host(const BatchPlan& bp, cudaStream_t st, const voi
   if (e == cudaSuccess) e = cudaEventRecord(bp.hev_done, sout);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(st, bp.hev_done, 0);
   return finish();
+}
+
+// ------------------------------------------------------- line registry
+// Lengths registered once per (device, direction, normalization): their
+// descriptors at fixed indices of two device arrays, their twiddles in one
+// device arena (offsets never move, so launches in flight are unaffected by
+// later registrations) and their Rader/Bluestein tables in allocations of
+// their own.
+constexpr uint32_t kRegLengths = 8192;
+constexpr uint64_t kRegTwiddles = 4ull << 20;  // complex values in the arena (32 MiB)
+
+struct LineRegistry {
+  int device = 0;
+  int32_t direction = B2F_FORWARD, normalization = B2F_NORM_INVERSE;
+  std::mutex mu;
+  std::map<uint64_t, int64_t> index;  // length -> descriptor index, -1 = not accepted
+  std::vector<std::unique_ptr<LenInfo>> infos;
+  BatchLen* d_lens = nullptr;
+  LongLenDesc* d_long_lens = nullptr;
+  c32* d_tw = nullptr;
+  uint64_t tw_used = 0;
+  std::vector<void*> tables;
+  uint64_t table_bytes = 0;
+  size_t cl_cap = 0;
+  int nsm = 148;
+  int cta_per_sm = 0, long_per_sm = 0;
+  size_t cta_smem_set = 0, long_smem_set = 0;
+  ~LineRegistry() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (void* p : tables) cudaFree(p);
+    cudaFree(d_lens);
+    cudaFree(d_long_lens);
+    cudaFree(d_tw);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// The twiddles one length reads (stage tables of its passes, the inter-pass
+// two-level table, the chirp tables), with offsets relative to `base`.
+static void length_twiddles(LenInfo& li, std::vector<cd>& tw, uint64_t base) {
+  std::map<uint32_t, uint32_t> cache;
+  BatchLen& d = li.d;
+  if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
+    LongLenDesc& g = li.lng;
+    attach_stage_table(li.s1, tw, cache);
+    attach_stage_table(li.s2, tw, cache);
+    for (int w = 0; w < 2; ++w) {
+      const Schedule& sc = w ? li.s2 : li.s1;
+      LongSched& ls = w ? g.s2 : g.s1;
+      ls.nst = sc.nst;
+      for (uint32_t k = 0; k < sc.nst; ++k) {
+        ls.st[k] = sc.st[k];
+        ls.st[k].tw_off += (uint32_t)base;
+      }
+    }
+    g.ta = (uint32_t)(base + tw.size());
+    for (uint32_t a = 0; a < g.N1; ++a) tw.push_back(root_fwd((uint64_t)a * g.N2, g.M));
+    g.tb = (uint32_t)(base + tw.size());
+    for (uint32_t c = 0; c < g.N2; ++c) tw.push_back(root_fwd(c, g.M));
+    if (g.blue) {
+      const uint64_t twoN = 2ull * g.N;
+      uint64_t B = (uint64_t)std::ceil(std::sqrt((double)twoN));
+      while (B * B < twoN) ++B;
+      g.ca = (uint32_t)(base + tw.size());
+      for (uint64_t a = 0; a * B < twoN; ++a) tw.push_back(root_fwd(a * B, twoN));
+      g.cb = (uint32_t)(base + tw.size());
+      for (uint64_t b = 0; b < B; ++b) tw.push_back(root_fwd(b, twoN));
+      g.dCB = make_fastdiv((uint32_t)B);
+    }
+    return;
+  }
+  attach_stage_table(d.sch, tw, cache);
+  for (uint32_t k = 0; k < d.sch.nst; ++k) d.sch.st[k].tw_off += (uint32_t)base;
+}
+
+LineRegistry* line_registry_new(int device, int32_t direction, int32_t normalization) {
+  std::unique_ptr<LineRegistry> r(new LineRegistry());
+  r->device = device;
+  r->direction = direction;
+  r->normalization = normalization;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaDeviceGetAttribute(&r->nsm, cudaDevAttrMultiProcessorCount, device);
+  r->cl_cap = (size_t)smem_optin;
+  const bool ok = cudaMalloc(&r->d_lens, kRegLengths * sizeof(BatchLen)) == cudaSuccess &&
+                  cudaMalloc(&r->d_long_lens, kRegLengths * sizeof(LongLenDesc)) == cudaSuccess &&
+                  cudaMalloc(&r->d_tw, kRegTwiddles * sizeof(c32)) == cudaSuccess;
+  if (prev >= 0) cudaSetDevice(prev);
+  if (!ok) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return r.release();
+}
+
+void line_registry_free(LineRegistry* reg) { delete reg; }
+
+uint64_t line_registry_bytes(const LineRegistry* reg) {
+  if (!reg) return 0;
+  return kRegLengths * (sizeof(BatchLen) + sizeof(LongLenDesc)) + kRegTwiddles * sizeof(c32) +
+         reg->table_bytes;
+}
+
+// Registers length n (lock held, device current); returns its index or -1.
+static int64_t registry_add(LineRegistry& r, uint64_t n) {
+  auto it = r.index.find(n);
+  if (it != r.index.end()) return it->second;
+  int64_t idx = -1;
+  std::unique_ptr<LenInfo> li(new LenInfo());
+  const size_t cta_cap = 44 * 1024;  // the batch kernels' four-CTA share of an SM
+  if (n >= 2 && n <= 0xFFFFFFFFull && r.infos.size() < kRegLengths &&
+      classify(n, r.direction, r.normalization, cta_cap, r.cl_cap, false, *li) &&
+      li->d.kind != BK_CL_MIXED && li->d.kind != BK_CL_BLUE) {
+    std::vector<cd> tw;
+    length_twiddles(*li, tw, r.tw_used);
+    bool ok = r.tw_used + tw.size() <= kRegTwiddles;
+    if (ok && !tw.empty()) {
+      std::vector<float> f(tw.size() * 2);
+      for (size_t i = 0; i < tw.size(); ++i) {
+        f[2 * i] = (float)tw[i].real();
+        f[2 * i + 1] = (float)tw[i].imag();
+      }
+      ok = cudaMemcpy(r.d_tw + r.tw_used, f.data(), f.size() * 4, cudaMemcpyHostToDevice) ==
+           cudaSuccess;
+    }
+    auto upload = [&](const void* src, size_t bytes, void** dst) -> bool {
+      if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
+      r.tables.push_back(*dst);
+      r.table_bytes += bytes;
+      return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (ok && !li->bhat.empty()) {
+      std::vector<float> f(li->bhat.size() * 2);
+      for (size_t i = 0; i < li->bhat.size(); ++i) {
+        f[2 * i] = (float)li->bhat[i].real();
+        f[2 * i + 1] = (float)li->bhat[i].imag();
+      }
+      void* p = nullptr;
+      ok = upload(f.data(), f.size() * 4, &p);
+      li->d.bhat = (const c32*)p;
+      li->lng.bhat = (const c32*)p;
+    }
+    if (ok && !li->pin.empty()) {
+      void *a = nullptr, *b = nullptr;
+      ok = upload(li->pin.data(), li->pin.size() * 4, &a) &&
+           upload(li->pout.data(), li->pout.size() * 4, &b);
+      li->d.perm_in = (const uint32_t*)a;
+      li->d.perm_out = (const uint32_t*)b;
+    }
+    if (ok) {
+      idx = (int64_t)r.infos.size();
+      LongLenDesc g = li->lng;
+      if (li->d.kind != BK_LONG && li->d.kind != BK_LONG_BLUE) std::memset(&g, 0, sizeof(g));
+      ok = cudaMemcpy(r.d_lens + idx, &li->d, sizeof(BatchLen), cudaMemcpyHostToDevice) ==
+               cudaSuccess &&
+           cudaMemcpy(r.d_long_lens + idx, &g, sizeof(LongLenDesc), cudaMemcpyHostToDevice) ==
+               cudaSuccess;
+      if (ok) {
+        r.tw_used += tw.size();
+        r.infos.push_back(std::move(li));
+      } else {
+        idx = -1;
+      }
+    }
+    if (!ok) cudaGetLastError();
+  }
+  r.index[n] = idx;
+  return idx;
+}
+
+bool line_registry_accepts(LineRegistry* reg, uint64_t n) {
+  if (!reg) return false;
+  std::lock_guard<std::mutex> lk(reg->mu);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != reg->device) cudaSetDevice(reg->device);
+  const bool ok = registry_add(*reg, n) >= 0;
+  if (prev >= 0 && prev != reg->device) cudaSetDevice(prev);
+  return ok;
+}
+
+b2f_status line_batch_run(LineRegistry* reg, cudaStream_t st, const uint64_t* lengths,
+                          const uint64_t* in_off, const uint64_t* out_off, uint64_t n,
+                          const void* in, void* out, uint64_t* device_bytes) {
+  if (device_bytes) *device_bytes = 0;
+  if (!reg || !lengths || !in_off || !out_off || !in || !out || n == 0)
+    return fail(B2F_ERR_INVALID_ARGUMENT, "empty or null line batch");
+  std::lock_guard<std::mutex> lk(reg->mu);
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != reg->device) cudaSetDevice(reg->device);
+  auto done = [&](b2f_status s) {
+    if (prev >= 0 && prev != reg->device) cudaSetDevice(prev);
+    return s;
+  };
+  // an error left by an unrelated earlier call of this thread must not be
+  // read back as this launch's (launch errors are read with cudaGetLastError)
+  cudaGetLastError();
+  // lines by descriptor index
+  std::map<int64_t, std::vector<uint64_t>> by_idx;
+  for (uint64_t i = 0; i < n; ++i) {
+    const int64_t idx = registry_add(*reg, lengths[i]);
+    if (idx < 0)
+      return done(fail(B2F_ERR_UNSUPPORTED_LENGTH,
+                       "UnsupportedLength { len: " + std::to_string(lengths[i]) +
+                           " } (not a batched-launch length)"));
+    by_idx[idx].push_back(i);
+  }
+  std::vector<BatchTask> cta;
+  std::vector<double> cta_cost;
+  std::vector<uint64_t> off_in, off_out;
+  std::vector<LongTask> lt[3];
+  uint64_t scratch = 0;
+  uint32_t buf_cta = 1, long_cap = 0;
+  for (auto& kv : by_idx) {
+    const LenInfo& li = *reg->infos[kv.first];
+    const BatchLen& d = li.d;
+    if (d.kind == BK_LONG || d.kind == BK_LONG_BLUE) {
+      const LongLenDesc& g = li.lng;
+      const uint32_t Gc = 1u << g.lgc, Gr = 1u << g.lgr;
+      long_cap = std::max(long_cap, std::max(g.N1 * (Gc + 1), g.N2 * (Gr + 1)));
+      for (uint64_t line : kv.second) {
+        const uint64_t sc = scratch;
+        scratch += g.M;
+        for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc)
+          lt[0].push_back(LongTask{in_off[line], sc, (uint32_t)kv.first, g0, out_off[line]});
+        for (uint32_t g0 = 0; g0 < g.N1; g0 += Gr)
+          lt[1].push_back(LongTask{in_off[line], sc, (uint32_t)kv.first, g0, out_off[line]});
+        if (g.blue)
+          for (uint32_t g0 = 0; g0 < g.N2; g0 += Gc)
+            lt[2].push_back(LongTask{in_off[line], sc, (uint32_t)kv.first, g0, out_off[line]});
+      }
+      continue;
+    }
+    buf_cta = std::max<uint32_t>(buf_cta, d.G * d.LD);
+    const uint32_t first = (uint32_t)off_in.size();
+    for (uint64_t line : kv.second) {
+      off_in.push_back(in_off[line]);
+      off_out.push_back(out_off[line]);
+    }
+    for (size_t s = 0; s < kv.second.size(); s += d.G) {
+      BatchTask t;
+      t.len = (uint32_t)kv.first;
+      t.first = first + (uint32_t)s;
+      t.count = (uint32_t)std::min<size_t>(d.G, kv.second.size() - s);
+      t.pad = 0;
+      cta.push_back(t);
+      cta_cost.push_back(li.cost * t.count);
+    }
+  }
+  // longest CTA tasks first; long tasks by kind and pass length
+  {
+    std::vector<size_t> idx(cta.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cta_cost[a] > cta_cost[b]; });
+    std::vector<BatchTask> o(cta.size());
+    for (size_t i = 0; i < idx.size(); ++i) o[i] = cta[idx[i]];
+    cta.swap(o);
+  }
+  for (int ph = 0; ph < 3; ++ph)
+    std::stable_sort(lt[ph].begin(), lt[ph].end(), [&](const LongTask& a, const LongTask& b) {
+      const LongLenDesc& ga = reg->infos[a.len]->lng;
+      const LongLenDesc& gb = reg->infos[b.len]->lng;
+      return std::make_pair(ga.blue, ph == 1 ? ga.N2 : ga.N1) <
+             std::make_pair(gb.blue, ph == 1 ? gb.N2 : gb.N1);
+    });
+  // one stream-ordered block: counters, CTA tasks, offsets, long tasks, scratch
+  auto align = [](uint64_t b) { return (b + 255) / 256 * 256; };
+  const uint64_t nlt = lt[0].size() + lt[1].size() + lt[2].size();
+  const uint64_t b_cnt = align(kBatchCounters * 4), b_cta = align(cta.size() * sizeof(BatchTask));
+  const uint64_t b_off = align(off_in.size() * 8), b_lt = align(nlt * sizeof(LongTask));
+  const uint64_t b_scr = align(scratch * 8);
+  const uint64_t total = b_cnt + b_cta + 2 * b_off + b_lt + b_scr;
+  char* blk = nullptr;
+  if (cudaMallocAsync((void**)&blk, total, st) != cudaSuccess) {
+    cudaGetLastError();
+    return done(fail(B2F_ERR_RESOURCE_ALLOCATION, "line batch allocation failed"));
+  }
+  if (device_bytes) *device_bytes = total;
+  unsigned int* counters = (unsigned int*)blk;
+  BatchTask* d_cta = (BatchTask*)(blk + b_cnt);
+  uint64_t* d_off_in = (uint64_t*)(blk + b_cnt + b_cta);
+  uint64_t* d_off_out = (uint64_t*)(blk + b_cnt + b_cta + b_off);
+  LongTask* d_lt = (LongTask*)(blk + b_cnt + b_cta + 2 * b_off);
+  c32* d_scr = (c32*)(blk + b_cnt + b_cta + 2 * b_off + b_lt);
+  std::vector<LongTask> lt_all;
+  lt_all.reserve(nlt);
+  for (int ph = 0; ph < 3; ++ph) lt_all.insert(lt_all.end(), lt[ph].begin(), lt[ph].end());
+  cudaError_t e = cudaMemsetAsync(counters, 0, kBatchCounters * 4, st);
+  if (e == cudaSuccess && !cta.empty())
+    e = cudaMemcpyAsync(d_cta, cta.data(), cta.size() * sizeof(BatchTask), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !off_in.empty()) {
+    e = cudaMemcpyAsync(d_off_in, off_in.data(), off_in.size() * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_off_out, off_out.data(), off_out.size() * 8, cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess && nlt)
+    e = cudaMemcpyAsync(d_lt, lt_all.data(), nlt * sizeof(LongTask), cudaMemcpyHostToDevice, st);
+  // the kernels' shared-memory limits, raised to the largest seen so far
+  const size_t smem_cta = 2 * (size_t)buf_cta * 8 + 2 * kBatchMaxG * 8;
+  const size_t smem_long = (3 * (size_t)long_cap + 2 * kLongTab) * 8;
+  if (e == cudaSuccess && !cta.empty() && smem_cta > reg->cta_smem_set) {
+    e = set_smem(k_batch_cta, smem_cta);
+    reg->cta_smem_set = smem_cta;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&reg->cta_per_sm, k_batch_cta, kCtaThreads, smem_cta);
+  }
+  if (e == cudaSuccess && nlt && smem_long > reg->long_smem_set) {
+    e = set_smem(k_long_pass<1>, smem_long);
+    if (e == cudaSuccess) e = set_smem(k_long_pass<2>, smem_long);
+    if (e == cudaSuccess) e = set_smem(k_long_pass<3>, smem_long);
+    reg->long_smem_set = smem_long;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&reg->long_per_sm, k_long_pass<2>, kLongThreads,
+                                                  smem_long);
+  }
+  if (e == cudaSuccess && !cta.empty()) {
+    BatchParams pt{};
+    pt.in = (const c32*)in;
+    pt.out = (c32*)out;
+    pt.lens = reg->d_lens;
+    pt.line_off = d_off_in;
+    pt.line_off_out = d_off_out;
+    pt.inverse = reg->direction == B2F_INVERSE ? 1u : 0u;
+    pt.tw = reg->d_tw;
+    pt.tasks = d_cta;
+    pt.ntasks = (uint32_t)cta.size();
+    pt.counter = counters;
+    const unsigned grid = (unsigned)std::min<uint64_t>(
+        (uint64_t)reg->nsm * std::max(reg->cta_per_sm, 1), cta.size());
+    k_batch_cta<<<grid, kCtaThreads, smem_cta, st>>>(pt, buf_cta);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && nlt) {
+    LongParams lp{};
+    lp.in = (const c32*)in;
+    lp.out = (c32*)out;
+    lp.scratch = d_scr;
+    lp.tw = reg->d_tw;
+    lp.lens = reg->d_long_lens;
+    lp.cap = long_cap;
+    lp.inverse = reg->direction == B2F_INVERSE ? 1u : 0u;
+    uint64_t first = 0;
+    for (uint32_t ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
+      const uint64_t count = lt[ph].size();
+      if (count) {
+        lp.tasks = d_lt + first;
+        lp.ntasks = (uint32_t)count;
+        lp.phase = ph + 1;
+        lp.counter = counters + 4 + ph;
+        const unsigned grid = (unsigned)std::min<uint64_t>(
+            (uint64_t)reg->nsm * std::max(reg->long_per_sm, 1), (count + kLongChunk - 1) / kLongChunk);
+        if (ph == 0) k_long_pass<1><<<grid, kLongThreads, smem_long, st>>>(lp);
+        else if (ph == 1) k_long_pass<2><<<grid, kLongThreads, smem_long, st>>>(lp);
+        else k_long_pass<3><<<grid, kLongThreads, smem_long, st>>>(lp);
+        e = cudaGetLastError();
+      }
+      first += count;
+    }
+  }
+  cudaFreeAsync(blk, st);
+  if (e != cudaSuccess)
+    return done(fail(B2F_ERR_DEVICE, std::string("line batch launch failed: ") + cudaGetErrorString(e)));
+  return done(B2F_OK);
 }
 
 }  // namespace b2f

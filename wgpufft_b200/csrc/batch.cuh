@@ -70,7 +70,8 @@ struct BatchParams {
   const c32* tw;         // stage and inter-pass twiddle tables (FP64-built, rounded once)
   const BatchLen* lens;
   const BatchTask* tasks;
-  const uint64_t* line_off;  // complex offset of each line (sorted order)
+  const uint64_t* line_off;  // complex offset of each line in `in` (sorted order)
+  const uint64_t* line_off_out;  // its offset in `out`, or null: the same as in `in`
   uint32_t ntasks;
   uint32_t inverse;
   unsigned int* counter;
@@ -103,7 +104,7 @@ FFT_D c32 tw2(const BatchParams& bp, const BatchLen& L, uint32_t j, uint32_t B) 
 }
 
 // --------------------------------------------------------------- CTA tasks
-FFT_D void batch_mixed(const BatchParams& bp, const BatchLen& L, const int64_t* base, uint32_t cnt,
+FFT_D void batch_mixed(const BatchParams& bp, const BatchLen& L, const int64_t* base, const int64_t* obase, uint32_t cnt,
                        c32* A, c32* B, uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<float>::value;
   const uint32_t N = L.N, LD = L.LD;
@@ -128,11 +129,11 @@ FFT_D void batch_mixed(const BatchParams& bp, const BatchLen& L, const int64_t* 
     c32 v = r[c * LD + pidx<PAD>(n)];
     v.re *= sc;
     v.im = inv ? -v.im * sc : v.im * sc;
-    bp.out[base[c] + n] = v;
+    bp.out[obase[c] + n] = v;
   }
 }
 
-FFT_D void batch_rader(const BatchParams& bp, const BatchLen& L, const int64_t* base, uint32_t cnt,
+FFT_D void batch_rader(const BatchParams& bp, const BatchLen& L, const int64_t* base, const int64_t* obase, uint32_t cnt,
                        c32* A, c32* B, c32* x0s, c32* X0s, uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<float>::value;
   const uint32_t P = L.N, P1 = L.M, LD = L.LD;
@@ -175,11 +176,11 @@ FFT_D void batch_rader(const BatchParams& bp, const BatchLen& L, const int64_t* 
     }
     v.re *= sc;
     v.im = inv ? -v.im * sc : v.im * sc;
-    bp.out[base[c] + n] = v;
+    bp.out[obase[c] + n] = v;
   }
 }
 
-FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* base, uint32_t cnt,
+FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* base, const int64_t* obase, uint32_t cnt,
                       c32* A, c32* B, uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<float>::value;
   const uint32_t N = L.N, M = L.M, LD = L.LD;
@@ -213,7 +214,7 @@ FFT_D void batch_blue(const BatchParams& bp, const BatchLen& L, const int64_t* b
     c32 v = cmul(w, chirp<float>(k, N));
     v.re *= sc;
     v.im = inv ? -v.im * sc : v.im * sc;
-    bp.out[base[c] + k] = v;
+    bp.out[obase[c] + k] = v;
   }
 }
 
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ Ba
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BatchLen s_len;
   __shared__ int64_t s_base[kBatchMaxG];
+  __shared__ int64_t s_obase[kBatchMaxG];
   __shared__ uint32_t s_task;
   uint32_t s_len_idx = 0xFFFFFFFFu;  // length descriptor currently in s_len (same in every thread)
   c32* A = reinterpret_cast<c32*>(smem_raw);
@@ -239,12 +241,17 @@ __global__ void __launch_bounds__(256, 4) k_batch_cta(const __grid_constant__ Ba
     const BatchTask task = bp.tasks[t];
     if (task.len != s_len_idx) copy_words(&s_len, bp.lens + task.len, tid, T);
     s_len_idx = task.len;
-    for (uint32_t c = tid; c < task.count; c += T) s_base[c] = (int64_t)bp.line_off[task.first + c];
+    for (uint32_t c = tid; c < task.count; c += T) {
+      s_base[c] = (int64_t)bp.line_off[task.first + c];
+      s_obase[c] = (int64_t)(bp.line_off_out ? bp.line_off_out : bp.line_off)[task.first + c];
+    }
     __syncthreads();
     switch (s_len.kind) {
-      case BK_MIXED: batch_mixed(bp, s_len, s_base, task.count, A, B, tid, T); break;
-      case BK_RADER: batch_rader(bp, s_len, s_base, task.count, A, B, x0s, X0s, tid, T); break;
-      case BK_BLUE: batch_blue(bp, s_len, s_base, task.count, A, B, tid, T); break;
+      case BK_MIXED: batch_mixed(bp, s_len, s_base, s_obase, task.count, A, B, tid, T); break;
+      case BK_RADER:
+        batch_rader(bp, s_len, s_base, s_obase, task.count, A, B, x0s, X0s, tid, T);
+        break;
+      case BK_BLUE: batch_blue(bp, s_len, s_base, s_obase, task.count, A, B, tid, T); break;
       default: break;
     }
     __syncthreads();

@@ -246,3 +246,21 @@ FFT_D uint32_t fdiv(uint32_t n, const FastDiv& f) {
   if (f.mul == 0) return n >> f.shift;
   return __umulhi(n, f.mul) >> f.shift;
 }
+
+// W_M^m (m < M) from a two-level table, m = a*L + b: A[a] * B[b], A[a] =
+// W_M^{aL} and B[b] = W_M^b each computed in FP64 and rounded once, so the
+// product carries about one more rounding than a single table entry.
+// m < 2^31 takes the fast division, larger m a 64-bit one.
+template <class S>
+FFT_D cpx<S> tw_two_level(const cpx<S>* __restrict__ A, const cpx<S>* __restrict__ B, uint64_t m,
+                          const FastDiv& dL) {
+  uint32_t a, b;
+  if (m < 0x80000000ull) {
+    a = fdiv((uint32_t)m, dL);
+    b = (uint32_t)m - a * dL.d;
+  } else {
+    a = (uint32_t)(m / dL.d);
+    b = (uint32_t)(m - (uint64_t)a * dL.d);
+  }
+  return cmul(A[a], B[b]);
+}

@@ -24,6 +24,14 @@ cudaError_t launch_blue_elem_t(const BlueElemParams&, cudaStream_t);
 
 template <class S>
 cudaError_t launch_real_elem_t(const RealElemParams&, cudaStream_t);
+template <class S>
+cudaError_t launch_small_volume_t(const SmallVolumeParams&, unsigned, size_t, cudaStream_t);
+
+cudaError_t launch_small_volume(Prec p, const SmallVolumeParams& prm, unsigned threads,
+                                size_t smem, cudaStream_t st) {
+  if (p != PREC_F32) return cudaErrorInvalidValue;
+  return launch_small_volume_t<float>(prm, threads, smem, st);
+}
 
 cudaError_t launch_real_elem(Prec p, const RealElemParams& prm, cudaStream_t st) {
   switch (p) {

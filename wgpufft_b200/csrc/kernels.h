@@ -47,6 +47,11 @@ struct LinesParams {
   LineIO io;
   FastDiv d_tw;         // division by io.tw_div
   uint64_t tw_store_M;
+  // PF_TW_STORE from tables (when tws_a is set): W_M^m = tws_a[m / L] *
+  // tws_b[m % L], L = d_tws.d, both tables built in FP64 and rounded once
+  const void* tws_a;
+  const void* tws_b;
+  FastDiv d_tws;
   double scale;
   Schedule sch;
 };
@@ -108,6 +113,25 @@ struct RealParams {
   Schedule sch;             // schedule of h (even N0) or N0 (odd N0)
 };
 
+// Small volumes (the crate's SmallVolumePlan, src/runtime/small_volume.rs:
+// 1-42, 223-272): every axis of a C2C volume of at most 4096 points in one
+// CTA and one HBM pass.  The CTA loads its volume into shared memory, runs
+// each axis over all of that axis's lines (gathered into lines of pitch LD,
+// transformed by the Stockham engine, scattered back) and stores it.
+constexpr int kSmallVolumeMaxRank = 3;
+constexpr uint32_t kSmallVolumeMaxPoints = 4096;
+struct SmallVolumeParams {
+  const void* in;
+  void* out;
+  const void* tw;  // stage twiddles of every axis (sch[a].st[s].tw_off into it)
+  uint32_t rank, V, flags, buf;  // V points per volume, buf = values per work buffer
+  uint32_t dims[kSmallVolumeMaxRank], strides[kSmallVolumeMaxRank], LD[kSmallVolumeMaxRank];
+  FastDiv dN[kSmallVolumeMaxRank], dS[kSmallVolumeMaxRank];
+  uint64_t nvol;
+  double scale;
+  Schedule sch[kSmallVolumeMaxRank];
+};
+
 // Per-precision launchers (kernels.cu).
 cudaError_t launch_lines(Prec p, const LinesParams& prm, unsigned grid, unsigned threads,
                          size_t smem, cudaStream_t st);
@@ -125,6 +149,8 @@ cudaError_t launch_c2r(Prec p, const RealParams& prm, unsigned grid, unsigned th
                        size_t smem, cudaStream_t st);
 cudaError_t launch_blue_elem(Prec p, const BlueElemParams& prm, cudaStream_t st);
 cudaError_t launch_real_elem(Prec p, const RealElemParams& prm, cudaStream_t st);
+cudaError_t launch_small_volume(Prec p, const SmallVolumeParams& prm, unsigned threads,
+                                size_t smem, cudaStream_t st);
 // out[i] = scale * (conj?) in[i] for n complex values (length-1 transforms).
 cudaError_t launch_scale_copy(Prec p, const void* in, void* out, uint64_t n, double scale,
                               bool conj, cudaStream_t st);

@@ -85,9 +85,11 @@ FFT_D void store_lines(const C<S>* sm, const LinesParams& p, const Group& g, uin
     if (c < g.nvalid) {
       C<S> v = sm[c * p.LD + pidx<PAD>(n)];
       if (fl & PF_TW_STORE) {
+        // row < M / N and n < N: the exponent stays below M
         const uint64_t row = fdiv((uint32_t)(g.c0 + c), p.d_tw);
-        const uint64_t m = (row * (uint64_t)n) % p.tw_store_M;
-        v = cmul(v, twiddle<S>(m, p.tw_store_M));
+        const uint64_t m = row * (uint64_t)n;
+        v = cmul(v, p.tws_a ? tw_two_level((const C<S>*)p.tws_a, (const C<S>*)p.tws_b, m, p.d_tws)
+                            : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
       }
       if (fl & PF_SCALE) v = cscale(v, sc);
       if (fl & PF_CONJ_OUT) v.im = -v.im;
@@ -499,6 +501,59 @@ __global__ void k_scale_copy(const C<S>* __restrict__ in, C<S>* __restrict__ out
   }
 }
 
+// ----------------------------------------------------------- small volume
+// One CTA per volume (src/runtime/small_volume.rs:1-42): the volume sits in
+// shared memory in its natural order; axis a's lines (outer o, inner c <
+// stride, point i at o*N*stride + i*stride + c) are gathered into the work
+// buffer at line l = o*stride + c, pitch LD, transformed by the Stockham
+// engine and scattered back, so the volume crosses HBM once.
+template <class S>
+__global__ void __launch_bounds__(256) k_small_volume(const __grid_constant__ SmallVolumeParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PAD = PadOf<S>::value;
+  C<S>* vol = reinterpret_cast<C<S>*>(smem_raw);
+  C<S>* A = vol + p.V;
+  C<S>* B = A + p.buf;
+  const uint32_t tid = threadIdx.x, T = blockDim.x, V = p.V;
+  const uint64_t base = (uint64_t)blockIdx.x * V;
+  const C<S>* __restrict__ in = (const C<S>*)p.in;
+  const bool conj_in = p.flags & PF_CONJ_IN;
+  for (uint32_t e = tid; e < V; e += T) {
+    C<S> v = in[base + e];
+    if (conj_in) v.im = -v.im;
+    vol[e] = v;
+  }
+  __syncthreads();
+  const C<S>* tw = (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr;
+#pragma unroll 1
+  for (uint32_t a = 0; a < p.rank; ++a) {
+    const uint32_t N = p.dims[a], s = p.strides[a], LD = p.LD[a];
+    const uint32_t lines = V / N;
+    // element e of the volume = (o, i, c): l = o*s + c
+    for (uint32_t e = tid; e < V; e += T) {
+      const uint32_t oi = fdiv(e, p.dS[a]), c = e - oi * s;
+      const uint32_t o = fdiv(oi, p.dN[a]), i = oi - o * N;
+      A[(o * s + c) * LD + pidx<PAD>(i)] = vol[e];
+    }
+    __syncthreads();
+    const C<S>* r = fft_lines_smem<S>(A, B, p.sch[a], lines, LD, tid, T, tw);
+    for (uint32_t e = tid; e < V; e += T) {
+      const uint32_t oi = fdiv(e, p.dS[a]), c = e - oi * s;
+      const uint32_t o = fdiv(oi, p.dN[a]), i = oi - o * N;
+      vol[e] = r[(o * s + c) * LD + pidx<PAD>(i)];
+    }
+    __syncthreads();
+  }
+  C<S>* __restrict__ out = (C<S>*)p.out;
+  const S sc = Scalar<S>::from_double(p.scale);
+  for (uint32_t e = tid; e < V; e += T) {
+    C<S> v = vol[e];
+    if (p.flags & PF_SCALE) v = cscale(v, sc);
+    if (p.flags & PF_CONJ_OUT) v.im = -v.im;
+    out[base + e] = v;
+  }
+}
+
 // --------------------------------------------------- templated launchers
 // Raises the dynamic shared memory limit of a kernel once per (kernel,
 // device); kernels are told apart by address, not by type.
@@ -527,6 +582,11 @@ static cudaError_t launch(K kernel, const P& prm, unsigned grid, unsigned thread
   return cudaGetLastError();
 }
 
+template <class S>
+cudaError_t launch_small_volume_t(const SmallVolumeParams& prm, unsigned threads, size_t smem,
+                                  cudaStream_t st) {
+  return launch(k_small_volume<S>, prm, (unsigned)prm.nvol, threads, smem, st);
+}
 template <class S>
 cudaError_t launch_lines_t(const LinesParams& prm, unsigned grid, unsigned threads, size_t smem,
                            cudaStream_t st) {

@@ -81,12 +81,13 @@ struct LongLenDesc {
 // that the kernel can prefetch it with asynchronous copies (no dependent
 // load of a line record).
 struct LongTask {
-  uint64_t base;     // complex offset of the line in the input and output buffers
+  uint64_t base;     // complex offset of the line in the input buffer
   uint64_t scratch;  // complex offset of its scratch region (M values)
   uint32_t len;      // index into the length table
   uint32_t g0;       // first column (column passes) or row (row passes) of the task
+  uint64_t obase;    // complex offset of the line in the output buffer
 };
-static_assert(sizeof(LongTask) == 24, "task records are copied as three 8-byte words");
+static_assert(sizeof(LongTask) == 32, "task records are copied as four 8-byte words");
 
 struct LongParams {
   const c32* in;
@@ -393,7 +394,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
     // out[k1 + N1 k2], k1 = g0 + l, from the last stage
     EpiRow e;
     e.ok = g0 + l < N1;
-    e.dst = p.out + ln.base + (e.ok ? g0 + l : 0);
+    e.dst = p.out + ln.obase + (e.ok ? g0 + l : 0);
     e.N1 = N1;
     e.sc = d.scale;
     e.inv = inv;
@@ -460,7 +461,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
       cw.init(n, S * N2, d.N, T + kTabTa, T + kTabTb, d);
-      c32* dst = p.out + ln.base + n;
+      c32* dst = p.out + ln.obase + n;
       const c32* sp = r + i0 * P + l;
       for (uint32_t n1 = i0; n1 < N1 && n < d.N; n1 += S) {
         c32 wv = *sp;
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
   // record of task k into s_task[k % 4]
   auto fetch_task = [&](uint32_t k) {
     const uint32_t t = task_of(k);
-    if (t != kNone && tid < 3)
+    if (t != kNone && tid < 4)
       cp_async8_zfill(reinterpret_cast<uint64_t*>(&s_task[k & 3]) + tid,
                       reinterpret_cast<const uint64_t*>(p.tasks + t) + tid, true);
   };

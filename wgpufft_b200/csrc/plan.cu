@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <sstream>
 
@@ -467,7 +468,7 @@ struct Builder {
 
   // Table pointers are patched after upload, by pass index and field.
   enum Field { F_LINES_TW, F_RADER_TW, F_BLUE_TW, F_REAL_TW, F_PERM_IN, F_PERM_OUT, F_RADER_BHAT,
-               F_BLUE_BHAT, F_BELEM_BHAT };
+               F_BLUE_BHAT, F_BELEM_BHAT, F_TWS_A, F_TWS_B, F_SVOL_TW };
   struct Patch {
     size_t table, pass;
     Field field;
@@ -501,6 +502,9 @@ struct Builder {
         case F_RADER_BHAT: ps.rader.bhat = ptr; break;
         case F_BLUE_BHAT: ps.blue.bhat = ptr; break;
         case F_BELEM_BHAT: ps.belem.bhat = ptr; break;
+        case F_TWS_A: ps.lines.tws_a = ptr; break;
+        case F_TWS_B: ps.lines.tws_b = ptr; break;
+        case F_SVOL_TW: ps.svol.tw = ptr; break;
       }
     }
   }
@@ -525,9 +529,13 @@ static bool try_pow2_pass(Builder& b, Pass& ps, uint64_t outer_n) {
   } else {
     return false;
   }
-  const uint32_t maxT = f32 ? 512 : 256;
   int E = 16;
   if (f32 && (N >= 4096 || (colmajor && N >= 1024))) E = 32;
+  // CTAs stay at 256 threads (up to about 128 registers a thread), so that
+  // two or more of them share an SM and one's loads overlap another's
+  // butterflies; column tiles of 8192-point lines keep 512 threads (two
+  // columns, 16-byte rows) rather than one 8-byte column
+  const uint32_t maxT = (colmajor && N > 4096) ? 512 : 256;
   const uint32_t TL = (uint32_t)(N / E);
   if (TL == 0 || TL > maxT) return false;
   const uint32_t LD = (uint32_t)(N + (N >> 4) + 1);
@@ -857,9 +865,22 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
     uint32_t fa = PF_CFIRST_LOAD | PF_CFIRST_STORE | PF_TW_STORE;
     if (inverse && first) fa |= PF_CONJ_IN;
     const char* lab = p2 ? "smooth-axis-phase1-fused-pow2-stage" : "smooth-axis-phase1-fused-smooth-stage";
+    const size_t pass_a = b.next_pass();
     b2f_status st = add_lines_pass(b, axis, N1, a, O, fa, 1.0, src, ws_buf, lab, "mixed");
     if (st) return st;
-    b.plan.passes.back().lines.tw_store_M = N;
+    LinesParams& lpa = b.plan.passes.back().lines;
+    lpa.tw_store_M = N;
+    if (b.plan.cfg.tuning.twiddle_table) {
+      // W_N^{n2 k1} from two tables of about sqrt(N) values each
+      uint64_t L = (uint64_t)std::sqrt((double)N);
+      while (L * L < N) ++L;
+      std::vector<cd> ta, tb;
+      for (uint64_t q = 0; q * L < N; ++q) ta.push_back(root_fwd(q * L, N));
+      for (uint64_t q = 0; q < L; ++q) tb.push_back(root_fwd(q, N));
+      b.set_table(pass_a, Builder::F_TWS_A, b.add_table(b.pack_complex(ta)));
+      b.set_table(pass_a, Builder::F_TWS_B, b.add_table(b.pack_complex(tb)));
+      lpa.d_tws = make_fastdiv((uint32_t)L);
+    }
   }
   {
     // pass B: rows n2 of each k1, stored transposed at k1 + N1*k2, ws -> out
@@ -989,6 +1010,72 @@ static b2f_status add_real_generic_c2r(Builder& b, uint64_t N0, uint64_t nlines,
   return B2F_OK;
 }
 
+// The small-volume route (src/runtime/small_volume.rs:223-272): an f32 C2C
+// plan over every axis of a rank-2 or rank-3 volume of at most 4096 points
+// whose axes are all 2,3,5,7,11,13-smooth, no forced Rader/Bluestein axis,
+// the automatic large route and fuse_small_volumes on.  One pass, one CTA
+// per volume.  Returns false when the configuration is not eligible.
+static bool try_small_volume(Builder& b, double scale, bool inverse) {
+  const Config& cfg = b.plan.cfg;
+  const Tuning& t = cfg.tuning;
+  const size_t rank = cfg.shape.size();
+  if (b.plan.prec != PREC_F32 || rank < 2 || rank > (size_t)kSmallVolumeMaxRank) return false;
+  std::vector<uint32_t> axes(cfg.axes.begin(), cfg.axes.end());
+  std::sort(axes.begin(), axes.end());
+  for (size_t i = 0; i < rank; ++i)
+    if (axes.size() != rank || axes[i] != i) return false;
+  if (!t.force_rader_axes.empty() || !t.force_bluestein_axes.empty() || t.large_route != 0 ||
+      !t.fuse_small_volumes || t.lines_per_block > 0 || t.threads_per_block > 0)
+    return false;
+  uint64_t V = 1;
+  for (auto n : cfg.shape) V *= n;
+  if (V > kSmallVolumeMaxPoints) return false;
+  Pass ps;
+  ps.kind = Pass::SMALL_VOLUME;
+  ps.label = "small-volume-stage";
+  ps.route = "mixed-radix";
+  ps.axis = -1;
+  ps.src = BUF_IN;
+  ps.dst = BUF_OUT;
+  SmallVolumeParams& sv = ps.svol;
+  sv.rank = (uint32_t)rank;
+  sv.V = (uint32_t)V;
+  sv.nvol = cfg.batch;
+  sv.scale = scale;
+  sv.flags = (inverse ? (PF_CONJ_IN | PF_CONJ_OUT) : 0u) | (scale != 1.0 ? PF_SCALE : 0u);
+  std::vector<cd> tw;
+  uint32_t buf = 0;
+  uint64_t stride = 1;
+  for (size_t a = 0; a < rank; ++a) {
+    const uint64_t N = cfg.shape[a];
+    std::vector<uint32_t> rad;
+    std::vector<cd> tw_a;
+    if (N < 2 || !b.make_schedule(N, sv.sch[a], rad, tw_a)) return false;
+    for (uint32_t st = 0; st < sv.sch[a].nst; ++st) sv.sch[a].st[st].tw_off += (uint32_t)tw.size();
+    tw.insert(tw.end(), tw_a.begin(), tw_a.end());
+    sv.dims[a] = (uint32_t)N;
+    sv.strides[a] = (uint32_t)stride;
+    sv.dN[a] = make_fastdiv((uint32_t)N);
+    sv.dS[a] = make_fastdiv((uint32_t)stride);
+    sv.LD[a] = b.ld_for(N);
+    buf = std::max<uint32_t>(buf, (uint32_t)(V / N) * sv.LD[a]);
+    ps.radices.insert(ps.radices.end(), rad.begin(), rad.end());
+    stride *= N;
+  }
+  sv.buf = buf;
+  ps.smem = ((size_t)V + 2 * (size_t)buf) * b.cb();
+  if (ps.smem > b.smem_budget) return false;
+  ps.threads = 256;
+  ps.grid = (unsigned)std::min<uint64_t>(cfg.batch, 0x7FFFFFFFull);
+  if (cfg.batch > 0x7FFFFFFFull) return false;
+  if (t.twiddle_table && !tw.empty()) {
+    sv.flags |= PF_TW_TABLE;
+    b.set_table(b.next_pass(), Builder::F_SVOL_TW, b.add_table(b.pack_complex(tw)));
+  }
+  b.plan.passes.push_back(ps);
+  return true;
+}
+
 Plan::~Plan() {
   int prev = -1;
   cudaGetDevice(&prev);
@@ -999,6 +1086,8 @@ Plan::~Plan() {
     if (p) cudaFree(p);
   if (inplace_copy) cudaFree(inplace_copy);
   if (last_done) cudaEventDestroy(last_done);
+  if (view_in) cudaFree(view_in);
+  if (view_out) cudaFree(view_out);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -1037,7 +1126,8 @@ static void build_diagnostics(Plan& plan) {
                      : p.kind == Pass::BLUESTEIN ? "bluestein" : p.kind == Pass::R2C ? "r2c"
                      : p.kind == Pass::C2R ? "c2r" : p.kind == Pass::BLUE_ELEM ? "bluestein-elementwise"
                      : p.kind == Pass::REAL_ELEM ? "real-elementwise"
-                     : p.kind == Pass::TC_DFT64 ? "tensor-core-dft" : "scale-copy";
+                     : p.kind == Pass::TC_DFT64 ? "tensor-core-dft"
+                     : p.kind == Pass::SMALL_VOLUME ? "small-volume" : "scale-copy";
     uint32_t G = (p.kind == Pass::LINES || p.kind == Pass::POW2) ? p.lines.G : p.kind == Pass::RADER ? p.rader.L.G
                : p.kind == Pass::BLUESTEIN ? p.blue.L.G : (p.kind == Pass::R2C || p.kind == Pass::C2R) ? p.real.G : 0;
     os << (i ? "," : "") << "{\"label\":\"" << json_escape(p.label) << "\",\"kind\":\"" << kind
@@ -1170,6 +1260,8 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
       ps.tc_table = b.add_table(std::move(tb));
       ps.tc_err = b.add_table(std::vector<unsigned char>(16, 0));
       plan->passes.push_back(ps);
+    } else if (try_small_volume(b, scale, inverse)) {
+      // every axis in one pass
     } else {
       for (size_t ai = 0; ai < cfg.axes.size(); ++ai) {
         const uint32_t a = cfg.axes[ai];
@@ -1247,8 +1339,9 @@ b2f_status create_plan(const Config& cfg_in, int32_t kind, int device, Plan** ou
     plan->shared_state = plan->workspace_total() > 0 || !plan->in_place_kernels;
     for (const Pass& ps : plan->passes)
       if (ps.kind == Pass::TC_DFT64) plan->shared_state = true;
-    if (plan->shared_state &&
-        cudaEventCreateWithFlags(&plan->last_done, cudaEventDisableTiming) != cudaSuccess) {
+    // every plan gets the event: executions through staged views share
+    // device memory even when the plan's own route does not
+    if (cudaEventCreateWithFlags(&plan->last_done, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       if (prev >= 0) cudaSetDevice(prev);
       return fail(B2F_ERR_DEVICE, "plan event creation failed");
@@ -1276,6 +1369,9 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != plan.device) cudaSetDevice(plan.device);
+  // launches report through cudaGetLastError: clear what an unrelated
+  // earlier call of this thread left there
+  cudaGetLastError();
   cudaError_t e = cudaSuccess;
   for (const Pass& p0 : plan.passes) {
     Pass p = p0;  // launch parameters take the caller's pointers
@@ -1325,6 +1421,11 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
         p.relem.out = dst;
         e = launch_real_elem(plan.prec, p.relem, st);
         break;
+      case Pass::SMALL_VOLUME:
+        p.svol.in = src;
+        p.svol.out = dst;
+        e = launch_small_volume(plan.prec, p.svol, p.threads, p.smem, st);
+        break;
       case Pass::TC_DFT64:
         e = launch_dft64_tc(src, dst, (const float*)plan.device_allocs[p.tc_table], p.tc_nlines,
                             p.tc_scale, p.tc_inverse, (unsigned int*)plan.device_allocs[p.tc_err],
@@ -1344,8 +1445,8 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
 // records a new one.  Executions recorded into a CUDA graph (the stream is
 // capturing) are ordered by the graph itself and skip the events.
 template <class F>
-static b2f_status ordered(const Plan& plan, cudaStream_t st, F&& f) {
-  if (!plan.shared_state || !plan.last_done) return f();
+static b2f_status ordered(const Plan& plan, cudaStream_t st, F&& f, bool force = false) {
+  if (!(plan.shared_state || force) || !plan.last_done) return f();
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
     cudaGetLastError();
@@ -1367,6 +1468,14 @@ static b2f_status ordered(const Plan& plan, cudaStream_t st, F&& f) {
 }
 
 static b2f_status execute_in_place_impl(const Plan& plan, cudaStream_t st, void* buf);
+
+b2f_status run_ordered(const Plan& plan, cudaStream_t st, const std::function<b2f_status()>& f) {
+  return ordered(plan, st, f, true);
+}
+
+b2f_status run_passes_unordered(const Plan& plan, cudaStream_t st, const void* in, void* out) {
+  return run_passes(plan, st, in, out);
+}
 
 b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint64_t in_bytes,
                         void* out, uint64_t out_bytes) {

@@ -2,6 +2,7 @@
 // selection and the pass list a plan executes.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -59,7 +60,8 @@ enum BufId : int {
 constexpr int kNumWorkspaces = 6;
 
 struct Pass {
-  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM, REAL_ELEM, TC_DFT64 } kind = LINES;
+  enum Kind { LINES, POW2, RADER, BLUESTEIN, R2C, C2R, SCALE_COPY, BLUE_ELEM, REAL_ELEM, TC_DFT64,
+              SMALL_VOLUME } kind = LINES;
   int pow2_E = 16;         // POW2: values per thread
   bool colmajor = false;   // POW2: adjacent lines first
   std::string label;  // stage label (diagnostics)
@@ -75,6 +77,7 @@ struct Pass {
   RealParams real{};
   BlueElemParams belem{};
   RealElemParams relem{};
+  SmallVolumeParams svol{};
   uint64_t copy_n = 0;
   double copy_scale = 1.0;
   bool copy_conj = false;
@@ -117,6 +120,10 @@ struct Plan {
   mutable std::mutex exec_mu;
   mutable cudaEvent_t last_done = nullptr;
   mutable bool last_done_recorded = false;
+  // staging buffers of executions through strided logical views (created
+  // on first use under copy_mu, kept until the plan is freed)
+  mutable void* view_in = nullptr;
+  mutable void* view_out = nullptr;
   std::string diag_json;
   ~Plan();
 };
@@ -134,6 +141,11 @@ b2f_status create_plan(const Config& cfg, int32_t kind, int device, Plan** out,
 b2f_status execute_plan(const Plan& plan, cudaStream_t st, const void* in, uint64_t in_bytes,
                         void* out, uint64_t out_bytes);
 b2f_status execute_plan_in_place(const Plan& plan, cudaStream_t st, void* buf, uint64_t bytes);
+// f() ordered after the plan's previous execution and before its next (the
+// plan's completion event), whatever the plan's route.
+b2f_status run_ordered(const Plan& plan, cudaStream_t st, const std::function<b2f_status()>& f);
+// The plan's passes from in to out (sizes already checked), not ordered.
+b2f_status run_passes_unordered(const Plan& plan, cudaStream_t st, const void* in, void* out);
 
 // Thread-local error detail.
 b2f_status fail(b2f_status code, const std::string& msg);
@@ -155,4 +167,7 @@ const char* axis_kind_name(AxisKind k);
 // Opaque handles of the C ABI (shared by the translation units that use them).
 struct b2f_config {
   b2f::Config cfg;
+};
+struct b2f_plan {
+  b2f::Plan* plan;
 };

@@ -136,8 +136,10 @@ FFT_D void reg_load_any(uint32_t R, C<S> (&v)[E], const C<S>* __restrict__ in, i
 template <class S, int R, int E>
 FFT_D void reg_store_global(const C<S> (&v)[E], C<S>* __restrict__ out, int64_t base, int64_t es,
                             uint32_t t, uint32_t TL, uint32_t Ns, uint32_t fl, S sc,
-                            uint64_t tw_row, uint64_t tw_M) {
+                            uint64_t tw_row, const LinesParams& p) {
   constexpr int NB = E / R;
+  const C<S>* __restrict__ ta = (const C<S>*)p.tws_a;
+  const C<S>* __restrict__ tb = (const C<S>*)p.tws_b;
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
     const uint32_t j = t + u * TL;
@@ -145,7 +147,10 @@ FFT_D void reg_store_global(const C<S> (&v)[E], C<S>* __restrict__ out, int64_t 
     for (int r = 0; r < R; ++r) {
       const uint32_t n = j + r * Ns;
       C<S> x = v[u * R + r];
-      if (fl & PF_TW_STORE) x = cmul(x, twiddle<S>((tw_row * n) % tw_M, tw_M));
+      // tw_row < M / N and n < N: the exponent stays below M
+      if (fl & PF_TW_STORE)
+        x = cmul(x, ta ? tw_two_level(ta, tb, tw_row * n, p.d_tws)
+                       : twiddle<S>((tw_row * n) % p.tw_store_M, p.tw_store_M));
       if (fl & PF_SCALE) x = cscale(x, sc);
       if (fl & PF_CONJ_OUT) x.im = -x.im;
       out[base + (int64_t)n * es] = x;
@@ -156,12 +161,12 @@ FFT_D void reg_store_global(const C<S> (&v)[E], C<S>* __restrict__ out, int64_t 
 template <class S, int E>
 FFT_D void reg_store_any(uint32_t R, const C<S> (&v)[E], C<S>* __restrict__ out, int64_t base,
                          int64_t es, uint32_t t, uint32_t TL, uint32_t Ns, uint32_t fl, S sc,
-                         uint64_t tw_row, uint64_t tw_M) {
+                         uint64_t tw_row, const LinesParams& p) {
   switch (R) {
-    case 2: reg_store_global<S, 2, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, tw_M); break;
-    case 4: reg_store_global<S, 4, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, tw_M); break;
-    case 8: reg_store_global<S, 8, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, tw_M); break;
-    default: reg_store_global<S, 16, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, tw_M); break;
+    case 2: reg_store_global<S, 2, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, p); break;
+    case 4: reg_store_global<S, 4, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, p); break;
+    case 8: reg_store_global<S, 8, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, p); break;
+    default: reg_store_global<S, 16, E>(v, out, base, es, t, TL, Ns, fl, sc, tw_row, p); break;
   }
 }
 
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(sizeof(C<S>) == 8 ? 512 : 256)
     if (valid) {
       const uint64_t row = (p.flags & PF_TW_STORE) ? fdiv((uint32_t)(g.c0 + c), p.d_tw) : 0;
       reg_store_any<S, E>(sl.R, v, (C<S>*)p.out, g.out0 + (int64_t)c * g.dl_out, p.io.out_es, t,
-                          TL, sl.Ns, p.flags, sc, row, p.tw_store_M);
+                          TL, sl.Ns, p.flags, sc, row, p);
     }
     return;
   }
@@ -224,7 +229,9 @@ __global__ void __launch_bounds__(sizeof(C<S>) == 8 ? 512 : 256)
       C<S> x = sm[cc * LD + pidx<PAD>(n)];
       if (fl & PF_TW_STORE) {
         const uint64_t row = fdiv((uint32_t)(g.c0 + cc), p.d_tw);
-        x = cmul(x, twiddle<S>((row * (uint64_t)n) % p.tw_store_M, p.tw_store_M));
+        const uint64_t m = row * (uint64_t)n;
+        x = cmul(x, p.tws_a ? tw_two_level((const C<S>*)p.tws_a, (const C<S>*)p.tws_b, m, p.d_tws)
+                            : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
       }
       if (fl & PF_SCALE) x = cscale(x, sc);
       if (fl & PF_CONJ_OUT) x.im = -x.im;

@@ -3,22 +3,30 @@
 // into a caller's encoder).
 //
 // Clients submit transforms of any configuration with their data in host
-// memory.  One scheduler thread owns the device side:
-//   - admission: a request is admitted when the device bytes it needs (its
-//     staging buffers, plus the workspace of the plan it runs on) fit the
-//     HBM budget next to everything already in flight; otherwise it waits
-//     until in-flight groups complete and release memory;
-//   - continuous batching: admitted requests with the same configuration
-//     are coalesced into one group and run as a single plan execution whose
-//     batch is the sum of theirs (batches are contiguous blocks, so the
-//     requests' buffers simply sit back to back); new arrivals join the next
-//     group while earlier groups are still on the GPU;
-//   - overlap: groups rotate over several streams, each group being
-//     host->device copies, the transform, device->host copies, then a
-//     stream-ordered free, so copies of one group overlap the kernels of
-//     another;
-//   - resident plans: plans (and their tables/workspaces) are cached by
-//     configuration and reused.
+// memory (copied in and out by the loop) or in device memory (transformed
+// where it lies).  One scheduler thread owns the device side:
+//   - two routes.  Line requests (1D complex f32 over axis 0, any length
+//     and batch, no tuning) of one direction and normalization are
+//     coalesced, whatever their lengths, into one batched launch of the
+//     mixed-length line kernels (linebatch.h): every line of every request
+//     of the group is a line of that launch.  Every other request runs on a
+//     resident plan of its configuration; requests of the same
+//     configuration are coalesced into one execution over their summed
+//     batch (batches are contiguous blocks, so the requests' buffers sit
+//     back to back in the staging buffers);
+//   - resident plans are keyed by configuration without the batch and by a
+//     power-of-two batch bucket: a group's batch B runs as the binary
+//     decomposition of B over at most 13 cached plans, so no group size
+//     builds a new plan once its buckets exist.  Plans count against the
+//     HBM budget and the least recently used ones are evicted (after their
+//     last execution has completed) when admission needs the room;
+//   - admission: a group is admitted when its device bytes (staging, the
+//     line launch's task lists and scratch, any new plan) fit the budget
+//     next to everything in flight and resident; otherwise it waits for
+//     in-flight groups to complete;
+//   - continuous batching: arrivals join the next group while earlier
+//     groups run; groups rotate over several streams so the copies of one
+//     overlap the kernels of another.
 // Completion is observed with events; waiting clients are woken, latency is
 // recorded from submission to completion.
 #include <algorithm>
@@ -26,6 +34,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -34,6 +43,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "linebatch.h"
 #include "plan.h"
 
 namespace b2f {
@@ -46,9 +56,11 @@ struct SReq {
   uint64_t id = 0;
   Config cfg;
   int32_t kind = B2F_C2C;
-  std::string key;
-  const void* host_in = nullptr;
-  void* host_out = nullptr;
+  std::string key;   // group key: the line route's (direction, normalization) or the configuration
+  bool line = false; // line route
+  bool device = false;  // buffers in device memory
+  const void* in = nullptr;
+  void* out = nullptr;
   uint64_t in_bytes = 0, out_bytes = 0;  // the request's own sizes
   double t_submit = 0, t_done = 0;
   int state = 0;  // 0 queued, 1 in flight, 2 done, 3 failed
@@ -56,9 +68,16 @@ struct SReq {
   std::string error;
 };
 
+struct SPlan {
+  std::unique_ptr<Plan> plan;
+  uint64_t bytes = 0;
+  cudaEvent_t last = nullptr;  // completion of its last group
+  bool used = false;
+  std::list<std::string>::iterator lru;
+};
+
 struct SGroup {
   std::vector<SReq*> reqs;
-  int stream = 0;
   cudaEvent_t done = nullptr;
   uint64_t bytes = 0;  // device bytes held until completion
 };
@@ -69,7 +88,22 @@ static std::string config_key(const Config& c, int32_t kind) {
   for (auto s : c.shape) os << s << ",";
   os << "|";
   for (auto a : c.axes) os << a << ",";
+  const Tuning& t = c.tuning;
+  os << "|" << t.lines_per_block << "," << t.threads_per_block << "," << t.twiddle_table << ","
+     << t.tensor_cores << "," << t.fuse_small_volumes << "," << t.rader_max_prime;
+  for (auto a : t.force_rader_axes) os << ",r" << a;
+  for (auto a : t.force_bluestein_axes) os << ",b" << a;
   return os.str();
+}
+
+// 1D complex f32 over axis 0 with default kernel tuning: the line route.
+static bool line_config(const Config& c, int32_t kind) {
+  const Tuning d;
+  const Tuning& t = c.tuning;
+  return kind == B2F_C2C && c.precision == B2F_F32 && c.shape.size() == 1 && c.axes.size() == 1 &&
+         c.axes[0] == 0 && t.force_rader_axes.empty() && t.force_bluestein_axes.empty() &&
+         t.lines_per_block == 0 && t.threads_per_block == 0 && t.tensor_cores == 0 &&
+         t.rader_max_prime == d.rader_max_prime;
 }
 
 struct Server {
@@ -77,6 +111,7 @@ struct Server {
   uint64_t budget = 0;
   int nstreams = 4;
   uint32_t max_group = 64;
+  uint64_t max_line_group_bytes = 512ull << 20;
   bool coalesce = true;
   std::vector<cudaStream_t> streams;
   std::mutex mu;
@@ -85,18 +120,19 @@ struct Server {
   std::deque<SReq*> queue;
   std::unordered_map<uint64_t, std::unique_ptr<SReq>> reqs;
   std::vector<SGroup> inflight;
-  uint64_t used = 0;
+  uint64_t used = 0;  // staging and launch bytes in flight
   uint64_t next_id = 1;
   int next_stream = 0;
-  // plan cache: key (with the total batch) -> plan
-  std::map<std::string, std::unique_ptr<Plan>> plans;
-  // per cached plan, the end of its last execution: a plan's workspace is
-  // shared by its executions, so one on another stream waits for it
-  std::map<const Plan*, cudaEvent_t> plan_done;
+  // resident plans: key -> plan, least recently used first in `lru`
+  std::map<std::string, SPlan> plans;
+  std::list<std::string> lru;
   uint64_t plan_bytes = 0;
+  // line registries per (direction, normalization)
+  LineRegistry* regs[2][4] = {};
   // statistics
   std::vector<double> lat;
-  uint64_t completed = 0, failed = 0, groups = 0, coalesced = 0, transforms = 0;
+  uint64_t completed = 0, failed = 0, groups = 0, line_groups = 0, coalesced = 0, transforms = 0;
+  uint64_t evictions = 0;
   double t_first = 0, t_last = 0;
   std::thread worker;
 
@@ -112,20 +148,71 @@ struct Server {
       cudaEventSynchronize(g.done);
       cudaEventDestroy(g.done);
     }
-    for (auto& kv : plan_done) cudaEventDestroy(kv.second);
+    for (auto& kv : plans)
+      if (kv.second.last) cudaEventDestroy(kv.second.last);
+    plans.clear();
+    for (auto& row : regs)
+      for (auto* r : row) line_registry_free(r);
     for (auto s : streams) cudaStreamDestroy(s);
   }
 
-  Plan* get_plan(const Config& cfg, int32_t kind, b2f_status* st) {
+  LineRegistry* registry(int32_t dir, int32_t norm) {
+    LineRegistry*& r = regs[dir & 1][norm & 3];
+    if (!r) r = line_registry_new(device, dir, norm);
+    return r;
+  }
+
+  uint64_t registry_bytes() const {
+    uint64_t b = 0;
+    for (auto& row : regs)
+      for (auto* r : row) b += line_registry_bytes(r);
+    return b;
+  }
+
+  // Evicts least recently used plans that no group in flight uses until
+  // `need` more bytes fit the budget (lock held).  Returns whether they fit.
+  bool make_room(uint64_t need) {
+    while (used + plan_bytes + registry_bytes() + need > budget && !lru.empty()) {
+      bool evicted = false;
+      for (auto it = lru.begin(); it != lru.end(); ++it) {
+        SPlan& sp = plans[*it];
+        if (sp.last && cudaEventQuery(sp.last) == cudaErrorNotReady) continue;
+        cudaGetLastError();
+        plan_bytes -= sp.bytes;
+        if (sp.last) cudaEventDestroy(sp.last);
+        const std::string k = *it;
+        lru.erase(it);
+        plans.erase(k);
+        ++evictions;
+        evicted = true;
+        break;
+      }
+      if (!evicted) break;
+    }
+    return used + plan_bytes + registry_bytes() + need <= budget;
+  }
+
+  // The resident plan of cfg (its batch already a bucket), created when new.
+  SPlan* get_plan(const Config& cfg, int32_t kind, b2f_status* st) {
     const std::string k = config_key(cfg, kind) + "|b" + std::to_string(cfg.batch);
     auto it = plans.find(k);
-    if (it != plans.end()) return it->second.get();
+    if (it != plans.end()) {
+      lru.erase(it->second.lru);
+      lru.push_back(k);
+      it->second.lru = std::prev(lru.end());
+      return &it->second;
+    }
     Plan* p = nullptr;
     *st = create_plan(cfg, kind, device, &p);
     if (*st) return nullptr;
-    plan_bytes += p->workspace_total() + p->table_bytes;
-    plans[k].reset(p);
-    return p;
+    SPlan& sp = plans[k];
+    sp.plan.reset(p);
+    sp.bytes = p->workspace_total() + p->table_bytes;
+    cudaEventCreateWithFlags(&sp.last, cudaEventDisableTiming);
+    lru.push_back(k);
+    sp.lru = std::prev(lru.end());
+    plan_bytes += sp.bytes;
+    return &sp;
   }
 
   // Completes every group whose event has fired (lock held).
@@ -161,76 +248,179 @@ struct Server {
     cv_done.notify_all();
   }
 
-  // Launches one group (lock held; the CUDA calls are asynchronous).
-  void launch(std::vector<SReq*>& members) {
-    SReq* r0 = members[0];
-    Config cfg = r0->cfg;
-    uint64_t total_batch = 0, in_total = 0, out_total = 0;
+  void fail_all(std::vector<SReq*>& members, b2f_status s, const std::string& msg) {
     for (SReq* r : members) {
-      total_batch += r->cfg.batch;
-      in_total += r->in_bytes;
-      out_total += r->out_bytes;
+      r->state = 3;
+      r->status = s;
+      r->error = msg;
+      ++failed;
     }
-    cfg.batch = total_batch;
-    b2f_status st = B2F_OK;
-    Plan* plan = get_plan(cfg, r0->kind, &st);
-    auto fail_all = [&](b2f_status s, const std::string& msg) {
-      for (SReq* r : members) {
-        r->state = 3;
-        r->status = s;
-        r->error = msg;
-        ++failed;
-      }
-      cv_done.notify_all();
-    };
-    if (!plan) {
-      fail_all(st, last_error());
-      return;
-    }
-    const int si = next_stream;
-    next_stream = (next_stream + 1) % nstreams;
-    cudaStream_t s = streams[si];
-    void* din = nullptr;
-    void* dout = nullptr;
-    if (cudaMallocAsync(&din, std::max<uint64_t>(in_total, 16), s) != cudaSuccess ||
-        cudaMallocAsync(&dout, std::max<uint64_t>(out_total, 16), s) != cudaSuccess) {
-      cudaGetLastError();
-      if (din) cudaFreeAsync(din, s);
-      fail_all(B2F_ERR_RESOURCE_ALLOCATION, "staging allocation failed");
-      return;
-    }
+    cv_done.notify_all();
+  }
+
+  // Copies the host requests' inputs into the staging buffer (device
+  // requests are used where they lie).
+  static cudaError_t copy_in(std::vector<SReq*>& members, char* din, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
     uint64_t off = 0;
     for (SReq* r : members) {
-      cudaMemcpyAsync((char*)din + off, r->host_in, r->in_bytes, cudaMemcpyHostToDevice, s);
+      if (!r->device && e == cudaSuccess)
+        e = cudaMemcpyAsync(din + off, r->in, r->in_bytes, cudaMemcpyHostToDevice, s);
       off += r->in_bytes;
     }
-    cudaEvent_t& pd = plan_done[plan];
-    if (!pd) cudaEventCreateWithFlags(&pd, cudaEventDisableTiming);
-    else cudaStreamWaitEvent(s, pd, 0);  // after this group's copies in are queued
-    st = execute_plan(*plan, s, din, in_total, dout, out_total);
-    if (pd) cudaEventRecord(pd, s);
-    off = 0;
+    return e;
+  }
+  static cudaError_t copy_out(std::vector<SReq*>& members, const char* dout, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    uint64_t off = 0;
     for (SReq* r : members) {
-      cudaMemcpyAsync(r->host_out, (char*)dout + off, r->out_bytes, cudaMemcpyDeviceToHost, s);
+      if (!r->device && e == cudaSuccess)
+        e = cudaMemcpyAsync(r->out, dout + off, r->out_bytes, cudaMemcpyDeviceToHost, s);
       off += r->out_bytes;
     }
-    cudaFreeAsync(din, s);
-    cudaFreeAsync(dout, s);
+    return e;
+  }
+
+  // A failed launch: nothing more is queued that touches the requests'
+  // memory, the stream finishes the copies it already holds, then the
+  // staging is freed and the requests are failed.
+  void abort_group(std::vector<SReq*>& members, cudaStream_t s, void* din, void* dout,
+                   b2f_status st, const std::string& msg) {
+    if (din) cudaFreeAsync(din, s);
+    if (dout) cudaFreeAsync(dout, s);
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    fail_all(members, st, msg);
+  }
+
+  // Runs one group on stream s (lock held; CUDA calls are asynchronous).
+  // Returns false when admission must wait for memory.
+  bool launch(std::vector<SReq*>& members) {
+    const int si = next_stream;
+    cudaStream_t s = streams[si];
+    uint64_t in_total = 0, out_total = 0;
+    bool all_device = true;
+    for (SReq* r : members) {
+      in_total += r->in_bytes;
+      out_total += r->out_bytes;
+      all_device = all_device && r->device;
+    }
+    const bool line = members[0]->line;
+    // staging for host requests (a group is all host or all device requests)
+    const bool stage = !all_device;
+    const uint64_t stage_bytes = stage ? in_total + out_total : 0;
+    if (line) {
+      // line lists and scratch: bounded by about twice the group's points
+      const uint64_t est = stage_bytes + 3 * in_total + (1u << 20);
+      if (!make_room(est)) return false;
+    } else if (!make_room(stage_bytes)) {
+      return false;
+    }
+    next_stream = (next_stream + 1) % nstreams;
+    char* din = nullptr;
+    char* dout = nullptr;
+    if (stage) {
+      if (cudaMallocAsync((void**)&din, std::max<uint64_t>(in_total, 16), s) != cudaSuccess ||
+          cudaMallocAsync((void**)&dout, std::max<uint64_t>(out_total, 16), s) != cudaSuccess) {
+        cudaGetLastError();
+        abort_group(members, s, din, nullptr, B2F_ERR_RESOURCE_ALLOCATION, "staging allocation failed");
+        return true;
+      }
+    }
+    cudaError_t e = stage ? copy_in(members, din, s) : cudaSuccess;
+    if (e != cudaSuccess) {
+      abort_group(members, s, din, dout, B2F_ERR_DEVICE, cudaGetErrorString(e));
+      return true;
+    }
+    b2f_status st = B2F_OK;
+    uint64_t extra = 0;
+    if (line) {
+      // every line of every request: (length, input offset, output offset)
+      // relative to the staging buffers or to the lowest request address
+      std::vector<uint64_t> lens, ioff, ooff;
+      uintptr_t ibase = UINTPTR_MAX, obase = UINTPTR_MAX;
+      if (!stage)
+        for (SReq* r : members) {
+          ibase = std::min(ibase, (uintptr_t)r->in);
+          obase = std::min(obase, (uintptr_t)r->out);
+        }
+      uint64_t off = 0;
+      for (SReq* r : members) {
+        const uint64_t N = r->cfg.shape[0];
+        const uint64_t i0 = stage ? off / 8 : ((uintptr_t)r->in - ibase) / 8;
+        const uint64_t o0 = stage ? off / 8 : ((uintptr_t)r->out - obase) / 8;
+        for (uint64_t b = 0; b < r->cfg.batch; ++b) {
+          lens.push_back(N);
+          ioff.push_back(i0 + b * N);
+          ooff.push_back(o0 + b * N);
+        }
+        off += r->in_bytes;
+      }
+      LineRegistry* reg = registry(members[0]->cfg.direction, members[0]->cfg.normalization);
+      st = reg ? line_batch_run(reg, s, lens.data(), ioff.data(), ooff.data(), lens.size(),
+                                stage ? (const void*)din : (const void*)ibase,
+                                stage ? (void*)dout : (void*)obase, &extra)
+               : fail(B2F_ERR_RESOURCE_ALLOCATION, "line registry allocation failed");
+      if (st == B2F_OK) ++line_groups;
+    } else {
+      // binary decomposition of the batch over bucketed resident plans
+      uint64_t in_off = 0, out_off = 0;
+      for (SReq* r : stage ? std::vector<SReq*>{members[0]} : members) {
+        Config cfg = r->cfg;
+        uint64_t left = 0;
+        if (stage)
+          for (SReq* q : members) left += q->cfg.batch;
+        else
+          left = cfg.batch;
+        const uint64_t per_in = (stage ? in_total : r->in_bytes) / left;
+        const uint64_t per_out = (stage ? out_total : r->out_bytes) / left;
+        const char* src = stage ? din : (const char*)r->in;
+        char* dst = stage ? dout : (char*)r->out;
+        uint64_t done_b = 0;
+        while (left > 0 && st == B2F_OK) {
+          uint64_t chunk = 1;
+          while (chunk * 2 <= left && chunk * 2 <= 4096) chunk *= 2;
+          cfg.batch = chunk;
+          SPlan* sp = get_plan(cfg, r->kind, &st);
+          if (!sp) break;
+          st = execute_plan(*sp->plan, s, src + done_b * per_in, chunk * per_in,
+                            dst + done_b * per_out, chunk * per_out);
+          cudaEventRecord(sp->last, s);
+          done_b += chunk;
+          left -= chunk;
+        }
+        in_off += r->in_bytes;
+        out_off += r->out_bytes;
+        if (st) break;
+      }
+    }
     if (st) {
-      fail_all(st, last_error());
-      return;
+      abort_group(members, s, din, dout, st, last_error());
+      return true;
+    }
+    e = stage ? copy_out(members, dout, s) : cudaSuccess;
+    if (stage) {
+      cudaFreeAsync(din, s);
+      cudaFreeAsync(dout, s);
     }
     SGroup g;
     g.reqs = members;
-    g.stream = si;
-    g.bytes = in_total + out_total;
+    g.bytes = stage_bytes + extra;
     cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
-    cudaEventRecord(g.done, s);
+    if (e == cudaSuccess) e = cudaEventRecord(g.done, s);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(s);
+      cudaGetLastError();
+      cudaEventDestroy(g.done);
+      fail_all(members, B2F_ERR_DEVICE, cudaGetErrorString(e));
+      return true;
+    }
     for (SReq* r : members) r->state = 1;
     used += g.bytes;
     ++groups;
     if (members.size() > 1) coalesced += members.size();
     inflight.push_back(g);
+    return true;
   }
 
   void run() {
@@ -241,12 +431,12 @@ struct Server {
                        [&] { return stop || !queue.empty() || !inflight.empty(); });
       if (stop && queue.empty() && inflight.empty()) break;
       reap(false);
-      // admit and group: take the queue head's configuration, then every
-      // other queued request with the same configuration (continuous batching)
+      // admit and group: the queue head's key, then every other queued
+      // request with the same key (continuous batching)
       while (!queue.empty()) {
         SReq* head = queue.front();
         std::vector<SReq*> members;
-        uint64_t need = 0;
+        uint64_t bytes = 0;
         for (auto it = queue.begin(); it != queue.end() && members.size() < max_group;) {
           SReq* r = *it;
           if (r->key != head->key || (!coalesce && !members.empty())) {
@@ -254,28 +444,31 @@ struct Server {
             continue;
           }
           const uint64_t b = r->in_bytes + r->out_bytes;
-          if (!members.empty() && used + need + b > budget) break;
+          if (!members.empty() && head->line && bytes + b > max_line_group_bytes) break;
+          if (!members.empty() && used + bytes + b > budget) break;
           members.push_back(r);
-          need += b;
+          bytes += b;
           it = queue.erase(it);
         }
-        if (used + need > budget && !inflight.empty()) {
+        if (bytes > budget) {
+          fail_all(members, B2F_ERR_RESOURCE_ALLOCATION,
+                   "request larger than the HBM admission budget");
+          continue;
+        }
+        if (!launch(members)) {
           // wait for memory: put them back in front, in order
           for (auto it = members.rbegin(); it != members.rend(); ++it) queue.push_front(*it);
+          if (inflight.empty()) {
+            SReq* r = queue.front();
+            queue.pop_front();
+            std::vector<SReq*> one{r};
+            fail_all(one, B2F_ERR_RESOURCE_ALLOCATION,
+                     "request does not fit the HBM admission budget next to the resident plans");
+            continue;
+          }
           reap(true);
           break;
         }
-        if (used + need > budget) {
-          for (SReq* r : members) {
-            r->state = 3;
-            r->status = B2F_ERR_RESOURCE_ALLOCATION;
-            r->error = "request larger than the HBM admission budget";
-            ++failed;
-          }
-          cv_done.notify_all();
-          continue;
-        }
-        launch(members);
         // bound the work in flight: at most two groups per stream
         if ((int)inflight.size() >= 2 * nstreams) reap(true);
       }
@@ -290,6 +483,65 @@ using namespace b2f;
 struct b2f_server {
   Server* s;
 };
+
+static b2f_status submit_any(b2f_server* srv, const b2f_config* cfg, int32_t kind, bool device,
+                             const void* in, uint64_t in_bytes, void* out, uint64_t out_bytes,
+                             uint64_t* request_id) {
+  if (!srv || !cfg || !in || !out || !request_id)
+    return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
+  b2f_status st = validate_config(cfg->cfg);
+  if (st) return st;
+  if (kind < B2F_C2C || kind > B2F_C2R) return fail(B2F_ERR_INVALID_ARGUMENT, "unknown kind");
+  const Config& c = cfg->cfg;
+  uint64_t total = c.batch, packed = c.batch;
+  for (size_t d = 0; d < c.shape.size(); ++d) {
+    total *= c.shape[d];
+    packed *= d == 0 ? c.shape[0] / 2 + 1 : c.shape[d];
+  }
+  const uint64_t cb = c.precision == B2F_F32 ? 8 : 16, sb = cb / 2;
+  uint64_t need_in = total * cb, need_out = total * cb;
+  if (kind == B2F_R2C) {
+    need_in = total * sb;
+    need_out = packed * cb;
+  } else if (kind == B2F_C2R) {
+    need_in = packed * cb;
+    need_out = total * sb;
+  }
+  if (in_bytes < need_in || out_bytes < need_out)
+    return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall: request buffers");
+  Server* s = srv->s;
+  std::unique_ptr<SReq> r(new SReq());
+  r->cfg = c;
+  r->kind = kind;
+  r->device = device;
+  r->line = line_config(c, kind) && (!device || ((uintptr_t)in % 8 == 0 && (uintptr_t)out % 8 == 0));
+  if (r->line) {
+    LineRegistry* reg;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      reg = s->registry(c.direction, c.normalization);
+    }
+    r->line = reg && line_registry_accepts(reg, c.shape[0]);
+  }
+  r->key = (r->line ? "lines|" + std::to_string(c.direction) + "|" + std::to_string(c.normalization)
+                    : config_key(c, kind)) +
+           (device ? "|dev" : "|host");
+  r->in = in;
+  r->out = out;
+  r->in_bytes = need_in;
+  r->out_bytes = need_out;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    r->t_submit = now_s();
+    if (s->t_first == 0) s->t_first = r->t_submit;
+    *request_id = r->id;
+    s->queue.push_back(r.get());
+    s->reqs[r->id] = std::move(r);
+  }
+  s->cv_work.notify_one();
+  return B2F_OK;
+}
 
 extern "C" {
 
@@ -326,48 +578,13 @@ void b2f_server_free(b2f_server* srv) {
 b2f_status b2f_server_submit(b2f_server* srv, const b2f_config* cfg, int32_t kind,
                              const void* host_in, uint64_t in_bytes, void* host_out,
                              uint64_t out_bytes, uint64_t* request_id) {
-  if (!srv || !cfg || !host_in || !host_out || !request_id)
-    return fail(B2F_ERR_INVALID_ARGUMENT, "null argument");
-  b2f_status st = validate_config(cfg->cfg);
-  if (st) return st;
-  if (kind < B2F_C2C || kind > B2F_C2R) return fail(B2F_ERR_INVALID_ARGUMENT, "unknown kind");
-  const Config& c = cfg->cfg;
-  uint64_t total = c.batch, packed = c.batch;
-  for (size_t d = 0; d < c.shape.size(); ++d) {
-    total *= c.shape[d];
-    packed *= d == 0 ? c.shape[0] / 2 + 1 : c.shape[d];
-  }
-  const uint64_t cb = c.precision == B2F_F32 ? 8 : 16, sb = cb / 2;
-  uint64_t need_in = total * cb, need_out = total * cb;
-  if (kind == B2F_R2C) {
-    need_in = total * sb;
-    need_out = packed * cb;
-  } else if (kind == B2F_C2R) {
-    need_in = packed * cb;
-    need_out = total * sb;
-  }
-  if (in_bytes < need_in || out_bytes < need_out)
-    return fail(B2F_ERR_BUFFER_TOO_SMALL, "BufferViewTooSmall: request buffers");
-  std::unique_ptr<SReq> r(new SReq());
-  r->cfg = c;
-  r->kind = kind;
-  r->key = config_key(c, kind);
-  r->host_in = host_in;
-  r->host_out = host_out;
-  r->in_bytes = need_in;
-  r->out_bytes = need_out;
-  Server* s = srv->s;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    r->id = s->next_id++;
-    r->t_submit = now_s();
-    if (s->t_first == 0) s->t_first = r->t_submit;
-    *request_id = r->id;
-    s->queue.push_back(r.get());
-    s->reqs[r->id] = std::move(r);
-  }
-  s->cv_work.notify_one();
-  return B2F_OK;
+  return submit_any(srv, cfg, kind, false, host_in, in_bytes, host_out, out_bytes, request_id);
+}
+
+b2f_status b2f_server_submit_device(b2f_server* srv, const b2f_config* cfg, int32_t kind,
+                                    const void* dev_in, uint64_t in_bytes, void* dev_out,
+                                    uint64_t out_bytes, uint64_t* request_id) {
+  return submit_any(srv, cfg, kind, true, dev_in, in_bytes, dev_out, out_bytes, request_id);
 }
 
 b2f_status b2f_server_wait(b2f_server* srv, uint64_t request_id, double timeout_s) {
@@ -417,13 +634,15 @@ b2f_status b2f_server_stats_json(b2f_server* srv, char* buf, uint64_t* len) {
     const double span = s->t_last > s->t_first ? s->t_last - s->t_first : 0.0;
     std::ostringstream os;
     os << "{\"completed\":" << s->completed << ",\"failed\":" << s->failed
-       << ",\"groups\":" << s->groups << ",\"coalesced_requests\":" << s->coalesced
+       << ",\"groups\":" << s->groups << ",\"line_groups\":" << s->line_groups
+       << ",\"coalesced_requests\":" << s->coalesced
        << ",\"transforms\":" << s->transforms << ",\"p50_ms\":" << pct(0.50) * 1e3
        << ",\"p99_ms\":" << pct(0.99) * 1e3 << ",\"max_ms\":" << (l.empty() ? 0.0 : l.back() * 1e3)
        << ",\"span_s\":" << span << ",\"requests_per_s\":" << (span > 0 ? s->completed / span : 0.0)
        << ",\"ffts_per_s\":" << (span > 0 ? s->transforms / span : 0.0)
-       << ",\"hbm_in_use_bytes\":" << s->used << ",\"hbm_budget_bytes\":" << s->budget
+       << ",\"hbm_in_flight_bytes\":" << s->used << ",\"hbm_budget_bytes\":" << s->budget
        << ",\"resident_plans\":" << s->plans.size() << ",\"plan_bytes\":" << s->plan_bytes
+       << ",\"plan_evictions\":" << s->evictions << ",\"line_registry_bytes\":" << s->registry_bytes()
        << ",\"streams\":" << s->nstreams << ",\"coalesce\":" << (s->coalesce ? "true" : "false")
        << "}";
     j = os.str();
@@ -443,7 +662,8 @@ void b2f_server_reset_stats(b2f_server* srv) {
   std::lock_guard<std::mutex> lk(srv->s->mu);
   Server* s = srv->s;
   s->lat.clear();
-  s->completed = s->failed = s->groups = s->coalesced = s->transforms = 0;
+  s->completed = s->failed = s->groups = s->line_groups = s->coalesced = s->transforms = 0;
+  s->evictions = 0;
   s->t_first = s->t_last = 0;
 }
 

@@ -238,8 +238,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       s_fail = 1;
       done = mbar_wait(cur ? mb1 : mb0, parity[cur]);  // second bounded wait before moving on
     }
-    parity[cur] ^= 1;
-    pending[cur] = false;
+    // still pending after both waits: the drain below waits for it once more
+    if (done) {
+      parity[cur] ^= 1;
+      pending[cur] = false;
+    }
     tc_fence_after();
     __syncthreads();
     if (s_fail) break;
@@ -268,9 +271,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     __syncthreads();  // the staging area becomes an operand buffer again
   }
-  // no MMA may still write tensor memory when it is freed
+  // no MMA may still write tensor memory when it is freed: every committed
+  // group is waited for (bounded); a group that never completes (a device
+  // fault: each wait allows about a second) is recorded in bit 1 of the
+  // error flag, which the host reports (b2f_plan_device_status), and the
+  // columns are freed regardless, since a CTA that kept them would stall
+  // every later allocation on its SM
   for (uint32_t b = 0; b < 2; ++b)
-    if (pending[b]) mbar_wait(b ? mb1 : mb0, parity[b]);
+    if (pending[b] && !mbar_wait(b ? mb1 : mb0, parity[b]) && tid == 0) atomicOr(err, 2u);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
