@@ -7,7 +7,9 @@ lines stored back to back (1.27 GB in, 1.27 GB out: larger than L2, so no
 flush is needed between steps).  One step = one batched launch over all
 20,000 lines (b2f_batch_execute).  Reported beside it:
   - plain per-plan: the same lines, one FftPlan per length, one
-    execute_checked per line (what a caller of the reference's plan API does);
+    execute_checked per line (what a caller of the reference's plan API
+    does), the 20,000 executions recorded once into a CUDA graph
+    (FftRecorder) and replayed, so no Python runs between them;
   - e2e: the batched step through the public API with the input copied from
     pinned host memory and the output copied back inside the timed region
     (b2f_batch_execute_host: ~32 MiB chunks whose copies overlap the transforms);
@@ -18,14 +20,20 @@ flush is needed between steps).  One step = one batched launch over all
     the measured HBM copy bandwidth, with the DRAM traffic of an ncu capture
     (profiles/) scaled to the full workload; the short-line CTA-queue kernel
     (k_batch_cta) beside it;
-  - serving: an open-loop Poisson request stream through the serving loop
-    against the plain per-request path (p50/p99 latency, FFTs/s);
-  - cpu_baseline: the planned CPU FFT (oracle/cpu_port.c, a C restatement of
-    the reference's CpuFftPlan structure) on a bounded sample of the lines.
+  - configs: every other benchmark configuration through the plain
+    per-plan path, each with its relative L2 error against an FP64 FFT;
+  - serving: open-loop Poisson request streams of the serving configuration
+    at 1k-200k requests/s through the serving loop against the plain
+    per-request path (FFTs/s, p50/p99 latency, coalescing counts);
+  - cpu_baseline: the faster of scipy.fft (pocketfft, every host core; the
+    stand-in for the reference's CpuFftPlan, whose rustfft backend cannot
+    be built here) and the planned C port of CpuFftPlan (oracle/cpu_port.c).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-Under torchrun every rank runs the whole workload on its own GPU (replicas,
-weak scaling); rank 0 prints one JSON line.
+Under torchrun the 20,000 lines are split into one contiguous run of about
+equal points per rank (strong scaling, no data-path collective); the
+value is all lines over the slowest rank's time; rank 0 prints one JSON
+line.
 """
 from __future__ import annotations
 

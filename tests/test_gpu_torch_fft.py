@@ -20,12 +20,19 @@ def _cplx(shape, dtype, seed):
 
 
 def _oracle_c2c(x, dims, inverse, norm):
-    """numpy-ordered array x, torch dims -> oracle over crate axes."""
+    """numpy-ordered array x, torch dims -> the unnormalised oracle over the
+    crate axes, scaled the way torch.fft scales (by the transformed
+    dimensions only)."""
     k = x.ndim
     shape = list(x.shape)[::-1]
     axes = sorted(k - 1 - (d % k) for d in dims)
-    y = O.c2c_nd_f64(x.reshape(-1), shape, axes=axes, inverse=inverse, normalization=NORMS[norm])
-    return y.reshape(x.shape)
+    y = O.c2c_nd_f64(x.reshape(-1), shape, axes=axes, inverse=inverse,
+                     normalization=O.NORM_NONE).reshape(x.shape)
+    n = int(np.prod([x.shape[d % k] for d in dims]))
+    mode = norm or "backward"
+    if mode == "ortho":
+        return y / np.sqrt(n)
+    return y / n if (mode == "backward") == inverse else y
 
 
 @pytest.mark.parametrize("shape,dims,norm", [((3, 1000), [-1], None), ((48, 64), [-2, -1], "ortho"),

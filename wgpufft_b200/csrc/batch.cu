@@ -276,9 +276,23 @@ static void set_long(LenInfo& li, uint64_t N, uint64_t T, uint64_t n1, bool blue
   g.lgr = long_lines_log2(g.N2);
   g.blue = blue ? 1u : 0u;
   g.scale = d.scale;
-  g.dN2 = make_fastdiv(g.N2);
   li.s1 = schedule_for(g.N1);
   li.s2 = schedule_for(g.N2);
+}
+
+// The two-level tables of a long line (appended to tw; offsets relative to
+// `base`): W_M^{512 a} (a < ceil(M / 512)) and W_M^b (b < 512) for the
+// inter-pass twiddle, and for Bluestein lines the chirp W_2N^{512 a} and
+// W_2N^b, so the kernel splits an exponent with a shift and a mask.
+static void long_split_tables(LongLenDesc& g, std::vector<cd>& tw, uint64_t base) {
+  auto two_level = [&](uint64_t M, uint32_t* ta, uint32_t* tb) {
+    *ta = (uint32_t)(base + tw.size());
+    for (uint64_t a = 0; a * kTabSplit < M; ++a) tw.push_back(root_fwd(a * kTabSplit, M));
+    *tb = (uint32_t)(base + tw.size());
+    for (uint64_t b = 0; b < kTabSplit && b < M; ++b) tw.push_back(root_fwd(b, M));
+  };
+  two_level(g.M, &g.ta, &g.tb);
+  if (g.blue) two_level(2ull * g.N, &g.ca, &g.cb);
 }
 
 // Chooses the execution of one distinct length.
@@ -420,12 +434,18 @@ static cudaError_t set_smem(K kernel, size_t smem) {
   // the attribute is per kernel for the whole process, shared by every
   // batch and line registry: always raise it to the device's limit, so no
   // later, smaller setting can make another object's launch fail
+  // (less the kernel's static shared memory)
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
-  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-    optin = (int)smem;
+  cudaFuncAttributes fa{};
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  const int room = optin - (int)fa.sharedSizeBytes;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              std::max<int>(optin, (int)smem));
+                              std::max<int>(room, (int)smem));
 }
 
 static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets, uint64_t nlines,
@@ -511,21 +531,7 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
           ls.nst = sc.nst;
           for (uint32_t k = 0; k < sc.nst; ++k) ls.st[k] = sc.st[k];
         }
-        g.ta = (uint32_t)tw.size();
-        for (uint32_t a = 0; a < g.N1; ++a) tw.push_back(root_fwd((uint64_t)a * g.N2, g.M));
-        g.tb = (uint32_t)tw.size();
-        for (uint32_t c = 0; c < g.N2; ++c) tw.push_back(root_fwd(c, g.M));
-        if (g.blue) {
-          // chirp W_2N^q, q = a B + b, B = ceil(sqrt(2N))
-          const uint64_t twoN = 2ull * g.N;
-          uint64_t B = (uint64_t)std::ceil(std::sqrt((double)twoN));
-          while (B * B < twoN) ++B;
-          g.ca = (uint32_t)tw.size();
-          for (uint64_t a = 0; a * B < twoN; ++a) tw.push_back(root_fwd(a * B, twoN));
-          g.cb = (uint32_t)tw.size();
-          for (uint64_t b = 0; b < B; ++b) tw.push_back(root_fwd(b, twoN));
-          g.dCB = make_fastdiv((uint32_t)B);
-        }
+        long_split_tables(g, tw, 0);
         continue;
       }
       attach_stage_table(d.sch, tw, cache);
@@ -1171,20 +1177,7 @@ static void length_twiddles(LenInfo& li, std::vector<cd>& tw, uint64_t base) {
         ls.st[k].tw_off += (uint32_t)base;
       }
     }
-    g.ta = (uint32_t)(base + tw.size());
-    for (uint32_t a = 0; a < g.N1; ++a) tw.push_back(root_fwd((uint64_t)a * g.N2, g.M));
-    g.tb = (uint32_t)(base + tw.size());
-    for (uint32_t c = 0; c < g.N2; ++c) tw.push_back(root_fwd(c, g.M));
-    if (g.blue) {
-      const uint64_t twoN = 2ull * g.N;
-      uint64_t B = (uint64_t)std::ceil(std::sqrt((double)twoN));
-      while (B * B < twoN) ++B;
-      g.ca = (uint32_t)(base + tw.size());
-      for (uint64_t a = 0; a * B < twoN; ++a) tw.push_back(root_fwd(a * B, twoN));
-      g.cb = (uint32_t)(base + tw.size());
-      for (uint64_t b = 0; b < B; ++b) tw.push_back(root_fwd(b, twoN));
-      g.dCB = make_fastdiv((uint32_t)B);
-    }
+    long_split_tables(g, tw, base);
     return;
   }
   attach_stage_table(d.sch, tw, cache);

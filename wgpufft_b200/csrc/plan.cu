@@ -839,7 +839,12 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
   }
   const bool p2 = (N & (N - 1)) == 0;
   b.need(out_buf, N * s * O * b.cb());
-  if (b.fits_one_cta(N)) {
+  // A long strided axis in one pass holds G*N values per CTA, so only two
+  // to four adjacent columns fit: rows of 16-32 bytes, strided far apart.
+  // Split into two passes of about sqrt(N), each a tile of many adjacent
+  // columns (rows of hundreds of bytes), once enough columns exist.
+  const bool split_strided = s >= 16 && N >= 2048;
+  if (b.fits_one_cta(N) && !split_strided) {
     b2f_status st = add_lines_pass(b, axis, N, io, outer_n, flags, scale, src, out_buf,
                                    p2 ? "fused-pow2-workgroup-stage" : "fused-smooth-workgroup-stage",
                                    "mixed");
@@ -853,6 +858,40 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
   if (!four_step_split(b, N, &N1, &N2))
     return fail(B2F_ERR_UNSUPPORTED_LENGTH,
                 "UnsupportedLength { len: " + std::to_string(N) + " } (no four-step split)");
+  // Very long contiguous lines: the balanced split's column pass (N1 >=
+  // 2048, stride N2) again holds only a few adjacent columns per CTA, so
+  // such lines take three passes instead: columns of N1 <= 256 (wide
+  // tiles), then each row of N2 = B*C as columns of B (stride C, C
+  // adjacent columns) and rows of C stored transposed.
+  uint64_t B3 = 0, C3 = 0;
+  if (s == 1 && N > (1ull << 22)) {
+    for (uint64_t d = 256; d >= 16; --d) {
+      if (N % d || !b.fits_one_cta(d)) continue;
+      uint64_t bb, cc;
+      if (four_step_split(b, N / d, &bb, &cc) && cc >= 16) {
+        N1 = d;
+        N2 = N / d;
+        B3 = bb;
+        C3 = cc;
+        break;
+      }
+    }
+  }
+  // W_M^{row * n} on the store of pass `idx` from two tables of about
+  // sqrt(M) values each
+  auto store_twiddles = [&](size_t idx, uint64_t M) {
+    LinesParams& lp = b.plan.passes[idx].lines;
+    lp.tw_store_M = M;
+    if (!b.plan.cfg.tuning.twiddle_table) return;
+    uint64_t L = (uint64_t)std::sqrt((double)M);
+    while (L * L < M) ++L;
+    std::vector<cd> ta, tb;
+    for (uint64_t q = 0; q * L < M; ++q) ta.push_back(root_fwd(q * L, M));
+    for (uint64_t q = 0; q < L; ++q) tb.push_back(root_fwd(q, M));
+    b.set_table(idx, Builder::F_TWS_A, b.add_table(b.pack_complex(ta)));
+    b.set_table(idx, Builder::F_TWS_B, b.add_table(b.pack_complex(tb)));
+    lp.d_tws = make_fastdiv((uint32_t)L);
+  };
   {
     // pass A: columns n1 (stride N2*s), W_N^{n2 k1} on store, src -> ws
     LineIO a{};
@@ -868,19 +907,44 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
     const size_t pass_a = b.next_pass();
     b2f_status st = add_lines_pass(b, axis, N1, a, O, fa, 1.0, src, ws_buf, lab, "mixed");
     if (st) return st;
-    LinesParams& lpa = b.plan.passes.back().lines;
-    lpa.tw_store_M = N;
-    if (b.plan.cfg.tuning.twiddle_table) {
-      // W_N^{n2 k1} from two tables of about sqrt(N) values each
-      uint64_t L = (uint64_t)std::sqrt((double)N);
-      while (L * L < N) ++L;
-      std::vector<cd> ta, tb;
-      for (uint64_t q = 0; q * L < N; ++q) ta.push_back(root_fwd(q * L, N));
-      for (uint64_t q = 0; q < L; ++q) tb.push_back(root_fwd(q, N));
-      b.set_table(pass_a, Builder::F_TWS_A, b.add_table(b.pack_complex(ta)));
-      b.set_table(pass_a, Builder::F_TWS_B, b.add_table(b.pack_complex(tb)));
-      lpa.d_tws = make_fastdiv((uint32_t)L);
-    }
+    store_twiddles(pass_a, N);
+  }
+  if (B3) {
+    // pass B1: in each row k1 (N2 = B3*C3 points, n2 = m1*C3 + m2), the
+    // columns m2 over m1 (stride C3), W_N2^{m2 j1} on store, in place on ws
+    LineIO c1{};
+    c1.inner_n = (uint32_t)C3;
+    c1.mid_n = (uint32_t)N1;
+    c1.in_es = c1.out_es = (int64_t)C3;
+    c1.in_inner = c1.out_inner = 1;
+    c1.in_mid = c1.out_mid = (int64_t)N2;
+    c1.in_outer = c1.out_outer = (int64_t)N;
+    c1.tw_div = 1;
+    const size_t pass_b1 = b.next_pass();
+    b2f_status st = add_lines_pass(b, axis, B3, c1, O, PF_CFIRST_LOAD | PF_CFIRST_STORE | PF_TW_STORE,
+                                   1.0, ws_buf, ws_buf, "smooth-axis-phase2a-column-stage", "mixed");
+    if (st) return st;
+    store_twiddles(pass_b1, N2);
+    // pass B2: rows m2 of C3 contiguous points for each (k1, j1), stored at
+    // k1 + N1*(j1 + B3*j2); lines of adjacent k1 share each output row
+    LineIO c2{};
+    c2.inner_n = (uint32_t)N1;
+    c2.mid_n = (uint32_t)B3;
+    c2.in_es = 1;
+    c2.out_es = (int64_t)(N1 * B3);
+    c2.in_inner = (int64_t)N2;
+    c2.out_inner = 1;
+    c2.in_mid = (int64_t)C3;
+    c2.out_mid = (int64_t)N1;
+    c2.in_outer = c2.out_outer = (int64_t)N;
+    uint32_t f2 = PF_CFIRST_STORE;
+    if (inverse && last) f2 |= PF_CONJ_OUT;
+    if (last && scale != 1.0) f2 |= PF_SCALE;
+    st = add_lines_pass(b, axis, C3, c2, O, f2, scale, ws_buf, out_buf,
+                        "smooth-axis-phase2b-row-stage", "mixed");
+    if (st) return st;
+    *cur = out_buf;
+    return B2F_OK;
   }
   {
     // pass B: rows n2 of each k1, stored transposed at k1 + N1*k2, ws -> out

@@ -71,12 +71,36 @@ def _c2c(x, s, dim, norm, inverse):
     x = x.contiguous()
     prec = w.FftPrecision.F64 if x.dtype == torch.complex128 else w.FftPrecision.F32
     k = x.dim()
+    out = torch.empty_like(x)
+    if sorted(dims) == list(range(k - len(dims), k)):
+        # trailing dimensions: the crate's shape is theirs (reversed), the
+        # leading dimensions its batch, and its normalisation (1 / the
+        # product of the shape) is torch's
+        t = len(dims)
+        shape = list(x.shape[k - t:])[::-1]
+        batch = 1
+        for d in x.shape[:k - t]:
+            batch *= int(d)
+        plan = _plan(w.FftTransformKind.C2c, shape, list(range(t)), batch, inverse, _NORM[norm],
+                     prec, x.device.index)
+        plan.execute_checked(torch.view_as_real(x), torch.view_as_real(out))
+        return out
+    # other subsets: the crate scales by its whole shape, torch by the
+    # transformed dimensions only, so the plan runs unnormalised and the
+    # scale is applied here
     shape = list(x.shape)[::-1]
     axes = sorted(k - 1 - d for d in dims)
-    plan = _plan(w.FftTransformKind.C2c, shape, axes, 1, inverse, _NORM[norm], prec,
+    plan = _plan(w.FftTransformKind.C2c, shape, axes, 1, inverse, w.Normalization.NONE, prec,
                  x.device.index)
-    out = torch.empty_like(x)
     plan.execute_checked(torch.view_as_real(x), torch.view_as_real(out))
+    n = 1
+    for d in dims:
+        n *= int(x.shape[d])
+    mode = norm or "backward"
+    if mode == "ortho":
+        out *= 1.0 / n ** 0.5
+    elif (mode == "backward") == inverse:
+        out *= 1.0 / n
     return out
 
 
