@@ -311,8 +311,13 @@ b2f_status b2f_server_submit_device(b2f_server* server, const b2f_config* cfg, i
                                     uint64_t out_bytes, uint64_t* request_id);
 /* Blocks until the request completed (or timeout_s passed; 0 = 1 hour). */
 b2f_status b2f_server_wait(b2f_server* server, uint64_t request_id, double timeout_s);
-/* Blocks until nothing is queued or in flight. */
+/* Blocks until nothing is queued or in flight (while dispatch is held,
+ * until it is released or timeout_s passes). */
 b2f_status b2f_server_drain(b2f_server* server, double timeout_s);
+/* hold != 0: requests are queued but not dispatched; hold == 0 releases
+ * them, coalesced, so a burst submitted between the two forms as few
+ * groups as its keys allow.  Closing the server dispatches what is queued. */
+void b2f_server_hold(b2f_server* server, int32_t hold);
 /* Completed/failed counts, groups, coalesced requests, p50/p99 latency
  * (submission to completion), requests/s and FFTs/s over the served span,
  * HBM in use, resident plans; same length convention as the plan's. */

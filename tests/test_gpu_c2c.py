@@ -37,6 +37,14 @@ def test_f32_bluestein_lengths(cuda, n):
     check_c2c(w.FftConfig.new(n).with_direction(INV), seed=n + 1)
 
 
+@pytest.mark.parametrize("n", [622423, 1268090])
+def test_f32_long_bluestein_lines(cuda, n):
+    # one line whose Bluestein convolution spans many CTAs (prime; 2*5*173*733):
+    # the chirp and spectrum passes spread one line over the whole grid
+    check_c2c(w.FftConfig.new(n), seed=n)
+    check_c2c(w.FftConfig.new(n).with_batch(2).with_direction(INV), seed=n + 1)
+
+
 @pytest.mark.parametrize("n", [15015, 16384, 65536, 1 << 20])
 def test_f32_long_axes(cuda, n):
     check_c2c(w.FftConfig.new(n).with_batch(2), seed=3)

@@ -62,7 +62,7 @@ def run_c2r(shape, batch, prec, z, norm=w.Normalization.Inverse):
 TOL = {F32: 2e-6, F64: 1e-14}
 
 SHAPES = [[4], [5], [16], [17 * 2], [30], [1024], [1025], [6, 5], [64, 32, 16], [3, 2],
-          [4096, 3], [9, 8, 7], [2048, 4]]
+          [4096, 3], [9, 8, 7], [2048, 4], [47487], [2011186]]
 
 
 @pytest.mark.parametrize("shape", SHAPES)

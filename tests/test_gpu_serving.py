@@ -103,9 +103,11 @@ def test_served_results_match_oracle(cuda):
     srv = w.FftServer(streams=2)
     cfg = w.FftConfig.new(2048).with_batch(4)
     # a burst: the inputs are ready first, then eight identical requests
-    # arrive back to back and are coalesced while their plan is built
+    # are queued while dispatch is held and released together
     ins, outs = zip(*[host_arrays(cfg, w.FftTransformKind.C2c, rng) for _ in range(8)])
+    srv.hold()
     ids = [srv.submit(cfg, w.FftTransformKind.C2c, hin, hout) for hin, hout in zip(ins, outs)]
+    srv.hold(False)
     srv.drain(60.0)
     for i, hin, hout in zip(ids, ins, outs):
         srv.wait(i, 10.0)
@@ -152,7 +154,9 @@ def test_lines_of_different_lengths_share_one_launch(cuda):
     batches = [5, 3, 2, 4, 8, 2, 1, 1, 1, 1, 64, 7]
     cfgs, ins, outs = _line_requests(rng, lengths, batches)
     srv = w.FftServer(streams=2)
+    srv.hold()
     ids = [srv.submit(c, w.FftTransformKind.C2c, i, o) for c, i, o in zip(cfgs, ins, outs)]
+    srv.hold(False)
     srv.drain(120.0)
     st = srv.stats()
     for i in ids:
@@ -188,10 +192,12 @@ def test_device_buffer_requests(cuda):
              (w.FftConfig.new_nd([32, 32, 32]), w.FftTransformKind.R2c),
              (w.FftConfig.new(1000).with_precision(w.FftPrecision.F64), w.FftTransformKind.C2c)]
     reqs = []
+    srv.hold()
     for cfg, kind in items * 2:
         hin, hout = host_arrays(cfg, kind, rng)
         din, dout = hin.cuda(), torch.zeros_like(hout).cuda()
         reqs.append((cfg, kind, hin, din, dout, srv.submit_device(cfg, kind, din, dout)))
+    srv.hold(False)
     for cfg, kind, hin, din, dout, rid in reqs:
         srv.wait(rid, 60.0)
         ref = alone(cfg, kind, hin)
@@ -216,4 +222,33 @@ def test_plan_buckets_bound_the_resident_plans(cuda):
         ref = O.c2c_nd_f64(x, [32, 24], batch=b)
         assert O.rel_l2(hout.numpy().view(np.complex64), ref) <= 2e-6
     assert srv.stats()["resident_plans"] <= 4
+    srv.close()
+
+
+def test_hold_releases_one_group_per_key(cuda):
+    # requests queued while dispatch is held form one group per key when
+    # released: three 1D f32 lengths (one line launch), two identical 2D
+    # requests (one plan execution) and one f64 request
+    rng = np.random.default_rng(10)
+    C2C = w.FftTransformKind.C2c
+    items = [w.FftConfig.new(1000).with_batch(2), w.FftConfig.new(4099),
+             w.FftConfig.new(20000), w.FftConfig.new_nd([32, 48]).with_batch(3),
+             w.FftConfig.new_nd([32, 48]).with_batch(3),
+             w.FftConfig.new(512).with_precision(w.FftPrecision.F64)]
+    srv = w.FftServer(streams=2)
+    srv.hold()
+    reqs = []
+    for cfg in items:
+        hin, hout = host_arrays(cfg, C2C, rng)
+        reqs.append((cfg, hin, hout, srv.submit(cfg, C2C, hin, hout)))
+    assert srv.stats()["completed"] == 0
+    srv.hold(False)
+    srv.drain(60.0)
+    st = srv.stats()
+    assert st["groups"] == 3 and st["line_groups"] == 1 and st["coalesced_requests"] == 5, st
+    for cfg, hin, hout, rid in reqs:
+        srv.wait(rid, 10.0)
+        prec = cfg.precision()
+        ref = alone(cfg, C2C, hin)
+        assert O.rel_l2(as_complex(hout.numpy(), prec), as_complex(ref, prec)) <= TOL[prec]
     srv.close()

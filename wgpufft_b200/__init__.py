@@ -122,6 +122,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_server_drain": (st, [vp, ctypes.c_double]),
         "b2f_server_stats_json": (st, [vp, ctypes.c_char_p, ctypes.POINTER(u64)]),
         "b2f_server_reset_stats": (None, [vp]),
+        "b2f_server_hold": (None, [vp, ctypes.c_int32]),
         "b2f_status_string": (ctypes.c_char_p, [st]),
         "b2f_last_error_message": (u64, [ctypes.c_char_p, u64]),
         "b2f_version": (ctypes.c_char_p, []),
@@ -713,6 +714,11 @@ class FftServer:
 
     def reset_stats(self) -> None:
         lib().b2f_server_reset_stats(self._ptr)
+
+    def hold(self, held: bool = True) -> None:
+        """b2f_server_hold: while held, requests queue without being
+        dispatched; releasing dispatches them coalesced."""
+        lib().b2f_server_hold(self._ptr, 1 if held else 0)
 
     def close(self):
         if self._ptr:

@@ -281,18 +281,23 @@ static void set_long(LenInfo& li, uint64_t N, uint64_t T, uint64_t n1, bool blue
 }
 
 // The two-level tables of a long line (appended to tw; offsets relative to
-// `base`): W_M^{512 a} (a < ceil(M / 512)) and W_M^b (b < 512) for the
-// inter-pass twiddle, and for Bluestein lines the chirp W_2N^{512 a} and
-// W_2N^b, so the kernel splits an exponent with a shift and a mask.
+// `base`) with rows of L = the power of two >= sqrt(M): W_M^{L a}
+// (a < ceil(M / L)) and W_M^b (b < L) for the inter-pass twiddle, and for
+// Bluestein lines the chirp W_2N likewise, so the kernel splits an exponent
+// with a shift and a mask (M <= 512 * 512 keeps both within 512 values).
 static void long_split_tables(LongLenDesc& g, std::vector<cd>& tw, uint64_t base) {
-  auto two_level = [&](uint64_t M, uint32_t* ta, uint32_t* tb) {
+  auto two_level = [&](uint64_t M, uint32_t* ta, uint32_t* tb, uint32_t* split) {
+    uint32_t sh = 0;
+    while ((1ull << (2 * sh)) < M) ++sh;
+    const uint64_t L = 1ull << sh;
+    *split = sh;
     *ta = (uint32_t)(base + tw.size());
-    for (uint64_t a = 0; a * kTabSplit < M; ++a) tw.push_back(root_fwd(a * kTabSplit, M));
+    for (uint64_t a = 0; a * L < M; ++a) tw.push_back(root_fwd(a * L, M));
     *tb = (uint32_t)(base + tw.size());
-    for (uint64_t b = 0; b < kTabSplit && b < M; ++b) tw.push_back(root_fwd(b, M));
+    for (uint64_t b = 0; b < L; ++b) tw.push_back(root_fwd(b, M));
   };
-  two_level(g.M, &g.ta, &g.tb);
-  if (g.blue) two_level(2ull * g.N, &g.ca, &g.cb);
+  two_level(g.M, &g.ta, &g.tb, &g.tsplit);
+  if (g.blue) two_level(2ull * g.N, &g.ca, &g.cb, &g.csplit);
 }
 
 // Chooses the execution of one distinct length.

@@ -117,25 +117,6 @@ template <class S>
 FFT_D cpx<S> cmul(cpx<S> a, cpx<S> b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
-// f32 complex values are one float2 pair: sm_100 executes the pair's
-// add, subtract and multiply-add as one packed FP32x2 instruction
-// (per-component results identical to the scalar round-to-nearest ones).
-#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
-FFT_D float2 as_f2(cpx<float> a) { return make_float2(a.re, a.im); }
-FFT_D cpx<float> operator+(cpx<float> a, cpx<float> b) {
-  const float2 r = __fadd2_rn(as_f2(a), as_f2(b));
-  return {r.x, r.y};
-}
-FFT_D cpx<float> operator-(cpx<float> a, cpx<float> b) {
-  const float2 r = __ffma2_rn(as_f2(b), make_float2(-1.0f, -1.0f), as_f2(a));
-  return {r.x, r.y};
-}
-FFT_D cpx<float> cmul(cpx<float> a, cpx<float> b) {
-  const float2 t = __fmul2_rn(make_float2(a.re, a.re), as_f2(b));
-  const float2 r = __ffma2_rn(make_float2(-a.im, a.im), make_float2(b.im, b.re), t);
-  return {r.x, r.y};
-}
-#endif
 
 // a * conj(b)
 template <class S>

@@ -416,18 +416,28 @@ __global__ void __launch_bounds__(512) k_c2r_odd(const __grid_constant__ RealPar
   });
 }
 
+// Elementwise passes walk (line, chunk) pairs: a block iteration covers
+// kElemChunk consecutive points of one line, so one long line spreads over
+// the whole grid and many short lines share it alike.
+constexpr uint32_t kElemChunk = 2048;
+
 template <class S>
 __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueElemParams p) {
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t N = p.N, M = p.M;
   const S sc = Scalar<S>::from_double(p.scale);
-  for (uint64_t l = blockIdx.x; l < p.nlines; l += gridDim.x) {
+  const uint32_t L = p.mode == BE_POST ? N : M;  // points per line this pass writes
+  const uint64_t cpl = (L + kElemChunk - 1) / kElemChunk;
+  for (uint64_t blk = blockIdx.x; blk < p.nlines * cpl; blk += gridDim.x) {
+    const uint64_t l = blk / cpl;
+    const uint32_t c0 = (uint32_t)(blk - l * cpl) * kElemChunk;
+    const uint32_t c1 = c0 + kElemChunk < L ? c0 + kElemChunk : L;
     const uint64_t o = l / p.s, i = l - o * p.s;
     const int64_t base = (int64_t)(o * (uint64_t)N * p.s + i);
     if (p.mode == BE_PRE) {
       const C<S>* __restrict__ in = (const C<S>*)p.in;
       C<S>* __restrict__ ws = (C<S>*)p.out + l * M;
-      for (uint32_t m = tid; m < M; m += T) {
+      for (uint32_t m = c0 + tid; m < c1; m += T) {
         C<S> v = czero<S>();
         if (m < N) {
           v = in[base + (int64_t)m * (int64_t)p.s];
@@ -439,7 +449,7 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
     } else if (p.mode == BE_MID) {
       C<S>* ws = (C<S>*)p.out + l * M;
       const C<S>* __restrict__ bhat = (const C<S>*)p.bhat;
-      for (uint32_t k = tid; k < M; k += T) {
+      for (uint32_t k = c0 + tid; k < c1; k += T) {
         C<S> v = cmul(ws[k], bhat[k]);
         v.im = -v.im;
         ws[k] = v;
@@ -447,7 +457,7 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
     } else {
       const C<S>* __restrict__ ws = (const C<S>*)p.in + l * M;
       C<S>* __restrict__ out = (C<S>*)p.out;
-      for (uint32_t k = tid; k < N; k += T) {
+      for (uint32_t k = c0 + tid; k < c1; k += T) {
         C<S> w = ws[k];
         w.im = -w.im;
         C<S> v = cmul(w, chirp<S>(k, N));
@@ -463,19 +473,24 @@ template <class S>
 __global__ void __launch_bounds__(256) k_real_elem(const __grid_constant__ RealElemParams p) {
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t N0 = p.N0, P = p.P;
-  for (uint64_t l = blockIdx.x; l < p.nlines; l += gridDim.x) {
+  const uint32_t L = p.mode == RE_PACK ? P : N0;  // points per line this pass writes
+  const uint64_t cpl = (L + kElemChunk - 1) / kElemChunk;
+  for (uint64_t blk = blockIdx.x; blk < p.nlines * cpl; blk += gridDim.x) {
+    const uint64_t l = blk / cpl;
+    const uint32_t c0 = (uint32_t)(blk - l * cpl) * kElemChunk;
+    const uint32_t c1 = c0 + kElemChunk < L ? c0 + kElemChunk : L;
     if (p.mode == RE_EXPAND) {
       const S* __restrict__ in = (const S*)p.in + l * N0;
       C<S>* __restrict__ out = (C<S>*)p.out + l * N0;
-      for (uint32_t n = tid; n < N0; n += T) out[n] = {in[n], Scalar<S>::zero()};
+      for (uint32_t n = c0 + tid; n < c1; n += T) out[n] = {in[n], Scalar<S>::zero()};
     } else if (p.mode == RE_PACK) {
       const C<S>* __restrict__ in = (const C<S>*)p.in + l * N0;
       C<S>* __restrict__ out = (C<S>*)p.out + l * P;
-      for (uint32_t k = tid; k < P; k += T) out[k] = in[k];
+      for (uint32_t k = c0 + tid; k < c1; k += T) out[k] = in[k];
     } else if (p.mode == RE_UNPACK) {
       const C<S>* __restrict__ in = (const C<S>*)p.in + l * P;
       C<S>* __restrict__ out = (C<S>*)p.out + l * N0;
-      for (uint32_t k = tid; k < N0; k += T) {
+      for (uint32_t k = c0 + tid; k < c1; k += T) {
         // X[k] for k < P; X[N0-k] = conj(X[k]) above; DC and Nyquist real
         C<S> v = (k < P) ? in[k] : conj(in[N0 - k]);
         if (k == 0 || 2 * k == N0) v.im = Scalar<S>::zero();
@@ -484,7 +499,7 @@ __global__ void __launch_bounds__(256) k_real_elem(const __grid_constant__ RealE
     } else {
       const C<S>* __restrict__ in = (const C<S>*)p.in + l * N0;
       S* __restrict__ out = (S*)p.out + l * N0;
-      for (uint32_t n = tid; n < N0; n += T) out[n] = in[n].re;
+      for (uint32_t n = c0 + tid; n < c1; n += T) out[n] = in[n].re;
     }
   }
 }
@@ -616,7 +631,9 @@ cudaError_t launch_c2r_t(const RealParams& prm, unsigned grid, unsigned threads,
 }
 template <class S>
 cudaError_t launch_blue_elem_t(const BlueElemParams& prm, cudaStream_t st) {
-  uint64_t blocks = prm.nlines < 148ull * 16 ? prm.nlines : 148ull * 16;
+  const uint64_t L = prm.mode == BE_POST ? prm.N : prm.M;
+  const uint64_t work = prm.nlines * ((L + kElemChunk - 1) / kElemChunk);
+  uint64_t blocks = work < 148ull * 16 ? work : 148ull * 16;
   if (blocks == 0) blocks = 1;
   k_blue_elem<S><<<(unsigned)blocks, 256, 0, st>>>(prm);
   return cudaGetLastError();
@@ -624,7 +641,9 @@ cudaError_t launch_blue_elem_t(const BlueElemParams& prm, cudaStream_t st) {
 
 template <class S>
 cudaError_t launch_real_elem_t(const RealElemParams& prm, cudaStream_t st) {
-  uint64_t blocks = prm.nlines < 148ull * 16 ? prm.nlines : 148ull * 16;
+  const uint64_t L = prm.mode == RE_PACK ? prm.P : prm.N0;
+  const uint64_t work = prm.nlines * ((L + kElemChunk - 1) / kElemChunk);
+  uint64_t blocks = work < 148ull * 16 ? work : 148ull * 16;
   if (blocks == 0) blocks = 1;
   k_real_elem<S><<<(unsigned)blocks, 256, 0, st>>>(prm);
   return cudaGetLastError();

@@ -50,8 +50,6 @@ static_assert(kLongChunk >= 3, "the prologue claims chunks 0 and 1 only");
 // W_2N^b (B = ceil(sqrt(2N)) <= 512) where the last two are
 constexpr uint32_t kTabSt = 0, kTabTa = 512, kTabTb = 1024;
 constexpr uint32_t kLongTab = 1536;
-// row width of the two-level twiddle and chirp tables (M <= 512 * 512)
-constexpr uint32_t kTabSplitLog2 = 9, kTabSplit = 1u << kTabSplitLog2;
 
 enum LongPassKind : uint32_t {
   LP_COL = 0,    // smooth line, column pass: x -> scratch
@@ -72,12 +70,12 @@ struct LongLenDesc {
   uint32_t blue;
   float scale;
   const c32* bhat;    // Bluestein: spectrum of the conjugate chirp / M, natural order
-  // two-level tables of kTabSplit-wide rows (offsets into the twiddle
-  // table): W_M^{j} = W_M^{kTabSplit a} * W_M^{b}, j = a kTabSplit + b,
-  // a < ceil(M / kTabSplit), b < kTabSplit; the Bluestein chirp
-  // W_2N^{q} likewise (2N <= M <= kTabSplit^2)
-  uint32_t ta, tb;
-  uint32_t ca, cb;
+  // two-level tables (offsets into the twiddle table) with rows of
+  // L = 2^tsplit >= sqrt(M): W_M^j = W_M^{L a} * W_M^b, j = a L + b,
+  // a < ceil(M / L) <= 512, b < L <= 512; the Bluestein chirp W_2N^q
+  // likewise with rows of 2^csplit >= sqrt(2N)
+  uint32_t ta, tb, tsplit;
+  uint32_t ca, cb, csplit;
   LongSched s1, s2;   // schedules of N1 (columns) and N2 (rows)
 };
 
@@ -126,10 +124,10 @@ FFT_D uint32_t long_kind(uint32_t phase, bool blue) {
   return LP_BCOL3;
 }
 
-// W^j from a two-level table: j = a*kTabSplit + b, value ta[a] * tb[b]
-// (a shift and a mask, no division).
-FFT_D c32 tw_two(const c32* __restrict__ tw, uint32_t ta, uint32_t tb, uint32_t j) {
-  return cmul(tw[ta + (j >> kTabSplitLog2)], tw[tb + (j & (kTabSplit - 1))]);
+// W^j from a two-level table with rows of 2^sh: j = a*2^sh + b, value
+// ta[a] * tb[b] (a shift and a mask, no division).
+FFT_D c32 tw_two(const c32* __restrict__ tw, uint32_t ta, uint32_t tb, uint32_t j, uint32_t sh) {
+  return cmul(tw[ta + (j >> sh)], tw[tb + (j & ((1u << sh) - 1))]);
 }
 
 // Where the last stage of a pass puts its results: back into shared memory
@@ -145,10 +143,10 @@ struct EpiCol {  // scratch[N2 pos + c] = v * W_M^{c pos}
   static constexpr bool active = true;
   c32* dst;  // scratch of the line + c
   const c32* T;
-  uint32_t N2, c;
+  uint32_t N2, c, sh;
   bool ok;
   FFT_D void operator()(uint32_t pos, c32 v) const {
-    if (ok) dst[(uint64_t)N2 * pos] = cmul(v, tw_two(T, kTabTa, kTabTb, c * pos));
+    if (ok) dst[(uint64_t)N2 * pos] = cmul(v, tw_two(T, kTabTa, kTabTb, c * pos, sh));
   }
 };
 struct EpiRow {  // out[k1 + N1 pos], scaled, conjugated back for inverse transforms
@@ -252,12 +250,15 @@ FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t t
 // two-level chirp table (q = a B + b: ca[a] * cb[b]), read through the
 // read-only cache (value_ldg) or from a shared-memory copy (value).
 struct ChirpWalk {
-  uint32_t q, u, dsq, u2, twoN;
+  uint32_t q, u, dsq, u2, twoN, sh, mask;
   const c32* ca;
   const c32* cb;
-  FFT_D void init(uint64_t n, uint32_t D, uint32_t N, const c32* ta, const c32* tb) {
+  FFT_D void init(uint64_t n, uint32_t D, uint32_t N, const c32* ta, const c32* tb,
+                  uint32_t split) {
     ca = ta;
     cb = tb;
+    sh = split;
+    mask = (1u << split) - 1;
     twoN = 2 * N;
     q = (uint32_t)((n * n) % twoN);
     u = (uint32_t)((2 * n * (uint64_t)D) % twoN);
@@ -273,13 +274,11 @@ struct ChirpWalk {
     if (u >= twoN) u -= twoN;
   }
   FFT_D c32 value_ldg() const {
-    const float2 x = __ldg(reinterpret_cast<const float2*>(ca + (q >> kTabSplitLog2)));
-    const float2 y = __ldg(reinterpret_cast<const float2*>(cb + (q & (kTabSplit - 1))));
+    const float2 x = __ldg(reinterpret_cast<const float2*>(ca + (q >> sh)));
+    const float2 y = __ldg(reinterpret_cast<const float2*>(cb + (q & mask)));
     return cmul(c32{x.x, x.y}, c32{y.x, y.y});
   }
-  FFT_D c32 value() const {
-    return cmul(ca[q >> kTabSplitLog2], cb[q & (kTabSplit - 1)]);
-  }
+  FFT_D c32 value() const { return cmul(ca[q >> sh], cb[q & mask]); }
 };
 
 FFT_D void copy_async(c32* dst, const c32* src, uint32_t n, uint32_t tid) {
@@ -298,12 +297,12 @@ FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongTask&
     const uint32_t nx = colk ? d.N1 : d.N2;
     copy_async(T + kTabSt, p.tw + sch.st[0].tw_off, nx - 1, tid);
     if (kind == LP_COL || kind == LP_BCOL1 || kind == LP_BMID) {
-      copy_async(T + kTabTa, p.tw + d.ta, (d.M + kTabSplit - 1) >> kTabSplitLog2, tid);
-      copy_async(T + kTabTb, p.tw + d.tb, d.M < kTabSplit ? d.M : kTabSplit, tid);
+      copy_async(T + kTabTa, p.tw + d.ta, (d.M + (1u << d.tsplit) - 1) >> d.tsplit, tid);
+      copy_async(T + kTabTb, p.tw + d.tb, 1u << d.tsplit, tid);
     } else if (kind == LP_BCOL3) {
       // the chirp tables (ceil(2N / B) <= B <= 512 values each) in their place
-      copy_async(T + kTabTa, p.tw + d.ca, (2 * d.N + kTabSplit - 1) >> kTabSplitLog2, tid);
-      copy_async(T + kTabTb, p.tw + d.cb, 2 * d.N < kTabSplit ? 2 * d.N : kTabSplit, tid);
+      copy_async(T + kTabTa, p.tw + d.ca, (2 * d.N + (1u << d.csplit) - 1) >> d.csplit, tid);
+      copy_async(T + kTabTb, p.tw + d.cb, 1u << d.csplit, tid);
     }
   }
   if (colk) {
@@ -358,7 +357,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
     if (c < N2) {
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N, p.tw + d.ca, p.tw + d.cb);
+      cw.init(n, S * N2, d.N, p.tw + d.ca, p.tw + d.cb, d.csplit);
       c32* dp = X + i0 * P + l;
       for (uint32_t i = i0; i < N1 && n < d.N; i += S) {
         c32 v = *dp;
@@ -381,6 +380,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
     e.c = g0 + l;
     e.ok = e.c < N2;
     e.dst = p.scratch + ln.scratch + (e.ok ? e.c : 0);
+    e.sh = d.tsplit;
     e.T = T;
     e.N2 = N2;
     ilv_fft(X, W, sch, lg, tid, T, e);
@@ -446,7 +446,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
       const c32* sp = r + lane * P + rr;
 #pragma unroll 4
       for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
-        row[n2] = cmul(*sp, tw_two(T, kTabTa, kTabTb, n2 * k1));
+        row[n2] = cmul(*sp, tw_two(T, kTabTa, kTabTb, n2 * k1, d.tsplit));
         sp += tpr * P;
       }
     }
@@ -456,7 +456,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
       const float sc = d.scale;
       uint32_t n = N2 * i0 + c;
       ChirpWalk cw;
-      cw.init(n, S * N2, d.N, T + kTabTa, T + kTabTb);
+      cw.init(n, S * N2, d.N, T + kTabTa, T + kTabTb, d.csplit);
       c32* dst = p.out + ln.obase + n;
       const c32* sp = r + i0 * P + l;
       for (uint32_t n1 = i0; n1 < N1 && n < d.N; n1 += S) {

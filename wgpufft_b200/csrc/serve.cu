@@ -117,6 +117,7 @@ struct Server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
+  bool held = false;  // b2f_server_hold: queue without dispatching
   std::deque<SReq*> queue;
   std::unordered_map<uint64_t, std::unique_ptr<SReq>> reqs;
   std::vector<SGroup> inflight;
@@ -216,10 +217,10 @@ struct Server {
   }
 
   // Completes every group whose event has fired (lock held).
-  void reap(bool block_one) {
+  void reap() {
     for (size_t i = 0; i < inflight.size();) {
       SGroup& g = inflight[i];
-      cudaError_t q = block_one && i == 0 ? cudaEventSynchronize(g.done) : cudaEventQuery(g.done);
+      cudaError_t q = cudaEventQuery(g.done);
       if (q == cudaErrorNotReady) {
         ++i;
         continue;
@@ -243,9 +244,21 @@ struct Server {
       used -= g.bytes;
       cudaEventDestroy(g.done);
       inflight.erase(inflight.begin() + i);
-      block_one = false;
     }
     cv_done.notify_all();
+  }
+
+  // Waits for the oldest group in flight with the lock released, so clients
+  // keep submitting (and the queue keeps filling for coalescing) while the
+  // scheduler is blocked on the device; then completes what has fired.
+  // Only this thread changes `inflight`, so the event stays valid.
+  void wait_oldest(std::unique_lock<std::mutex>& lk) {
+    if (inflight.empty()) return;
+    cudaEvent_t ev = inflight.front().done;
+    lk.unlock();
+    cudaEventSynchronize(ev);
+    lk.lock();
+    reap();
   }
 
   void fail_all(std::vector<SReq*>& members, b2f_status s, const std::string& msg) {
@@ -305,7 +318,9 @@ struct Server {
       out_total += r->out_bytes;
       all_device = all_device && r->device;
     }
-    const bool line = members[0]->line;
+    // a line group of one request gains nothing from the batched line
+    // launch: it runs on its resident plan (fewer launches, no task lists)
+    const bool line = members[0]->line && members.size() > 1;
     // staging for host requests (a group is all host or all device requests)
     const bool stage = !all_device;
     const uint64_t stage_bytes = stage ? in_total + out_total : 0;
@@ -428,12 +443,12 @@ struct Server {
     std::unique_lock<std::mutex> lk(mu);
     while (true) {
       cv_work.wait_for(lk, std::chrono::microseconds(200),
-                       [&] { return stop || !queue.empty() || !inflight.empty(); });
+                       [&] { return stop || (!queue.empty() && !held) || !inflight.empty(); });
       if (stop && queue.empty() && inflight.empty()) break;
-      reap(false);
+      reap();
       // admit and group: the queue head's key, then every other queued
       // request with the same key (continuous batching)
-      while (!queue.empty()) {
+      while (!queue.empty() && (!held || stop)) {
         SReq* head = queue.front();
         std::vector<SReq*> members;
         uint64_t bytes = 0;
@@ -455,6 +470,7 @@ struct Server {
                    "request larger than the HBM admission budget");
           continue;
         }
+
         if (!launch(members)) {
           // wait for memory: put them back in front, in order
           for (auto it = members.rbegin(); it != members.rend(); ++it) queue.push_front(*it);
@@ -466,11 +482,11 @@ struct Server {
                      "request does not fit the HBM admission budget next to the resident plans");
             continue;
           }
-          reap(true);
+          wait_oldest(lk);
           break;
         }
         // bound the work in flight: at most two groups per stream
-        if ((int)inflight.size() >= 2 * nstreams) reap(true);
+        if ((int)inflight.size() >= 2 * nstreams) wait_oldest(lk);
       }
     }
   }
@@ -620,6 +636,15 @@ b2f_status b2f_server_drain(b2f_server* srv, double timeout_s) {
       return fail(B2F_ERR_DEVICE, "timed out draining the server");
   }
   return B2F_OK;
+}
+
+void b2f_server_hold(b2f_server* srv, int32_t hold) {
+  if (!srv) return;
+  {
+    std::lock_guard<std::mutex> lk(srv->s->mu);
+    srv->s->held = hold != 0;
+  }
+  srv->s->cv_work.notify_all();
 }
 
 b2f_status b2f_server_stats_json(b2f_server* srv, char* buf, uint64_t* len) {
