@@ -288,7 +288,8 @@ b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_
  * lengths into one batched launch of the mixed-length line kernels; other
  * requests of the same configuration are coalesced into one execution of a
  * resident plan (plans keyed by configuration and a power-of-two batch
- * bucket, evicted least recently used when the budget needs the room).
+ * bucket, or by the exact batch once a batch recurs; evicted least recently
+ * used when the budget needs the room).  A lone 1D request runs on a plan.
  * Requests carry host buffers (pinned memory lets the copies overlap;
  * results are written back to host_out) or device buffers
  * (b2f_server_submit_device).  When a group fails, no copy touching a

@@ -326,11 +326,21 @@ class FftConfig:
     def __len__(self):
         return self._shape[0] if self._shape else 0
 
+    _FIELDS = ("_shape", "_axes", "_batch", "_direction", "_normalization", "_precision",
+               "_tuning")
+
     def __eq__(self, other):
-        return isinstance(other, FftConfig) and self.__dict__ == other.__dict__
+        return isinstance(other, FftConfig) and all(
+            getattr(self, f) == getattr(other, f) for f in self._FIELDS)
 
     def _handle(self) -> "_ConfigHandle":
-        return _ConfigHandle(self)
+        # the native b2f_config of this (immutable) configuration, built on
+        # first use and kept for the object's lifetime
+        h = self.__dict__.get("_native")
+        if h is None:
+            h = _ConfigHandle(self)
+            self.__dict__["_native"] = h
+        return h
 
     def validate(self) -> None:
         with self._handle() as h:
@@ -362,7 +372,7 @@ class FftConfig:
 
 
 class _ConfigHandle:
-    """A b2f_config built from an FftConfig for the duration of one call."""
+    """The b2f_config built from an FftConfig (freed with the handle)."""
 
     def __init__(self, cfg: FftConfig):
         L = lib()
@@ -388,7 +398,14 @@ class _ConfigHandle:
         return self
 
     def __exit__(self, *exc):
-        lib().b2f_config_free(self.ptr)
+        return False
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().b2f_config_free(self.ptr)
+        except Exception:
+            pass
         self.ptr = None
 
 

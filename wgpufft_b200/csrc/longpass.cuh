@@ -105,13 +105,6 @@ struct LongParams {
   unsigned int* counter;  // work queue: chunks of kLongChunk tasks handed out in order
 };
 
-// cp.async of 8 bytes, zero-filled (nothing read) when !valid.
-FFT_D void cp_async8_zfill(void* smem, const void* gmem, bool valid) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  const unsigned n = valid ? 8u : 0u;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
-               : "memory");
-}
 FFT_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 FFT_D void cp_async_wait() {
@@ -131,13 +124,16 @@ FFT_D c32 tw_two(const c32* __restrict__ tw, uint32_t ta, uint32_t tb, uint32_t 
 }
 
 // Where the last stage of a pass puts its results: back into shared memory
-// (EpiNone), or straight from registers to global memory, value v of line l
-// at position pos: the column pass's scratch store with the inter-pass
-// twiddle (EpiCol), the row pass's output store (EpiRow).  A half-warp holds
-// one position of 16 lines, so each store is one G-value segment.
+// (EpiNone), or straight from registers to global memory, the R outputs
+// v[r] of one butterfly of line l at positions o + r*Ns: the column pass's
+// scratch store with the inter-pass twiddle (EpiCol), the row pass's output
+// store (EpiRow).  Addresses and twiddle exponents advance by a fixed step
+// per output.  A half-warp holds one position of 16 lines, so each store is
+// one G-value segment.
 struct EpiNone {
   static constexpr bool active = false;
-  FFT_D void operator()(uint32_t, c32) const {}
+  template <int R>
+  FFT_D void store(uint32_t, uint32_t, const c32*) const {}
 };
 struct EpiCol {  // scratch[N2 pos + c] = v * W_M^{c pos}
   static constexpr bool active = true;
@@ -145,21 +141,36 @@ struct EpiCol {  // scratch[N2 pos + c] = v * W_M^{c pos}
   const c32* T;
   uint32_t N2, c, sh;
   bool ok;
-  FFT_D void operator()(uint32_t pos, c32 v) const {
-    if (ok) dst[(uint64_t)N2 * pos] = cmul(v, tw_two(T, kTabTa, kTabTb, c * pos, sh));
+  template <int R>
+  FFT_D void store(uint32_t o, uint32_t Ns, const c32* v) const {
+    if (!ok) return;
+    uint32_t e = c * o;  // c * pos < M
+    const uint32_t de = c * Ns;
+    c32* dp = dst + (uint64_t)N2 * o;
+    const uint64_t step = (uint64_t)N2 * Ns;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      *dp = cmul(v[r], tw_two(T, kTabTa, kTabTb, e, sh));
+      e += de;
+      dp += step;
+    }
   }
 };
 struct EpiRow {  // out[k1 + N1 pos], scaled, conjugated back for inverse transforms
   static constexpr bool active = true;
   c32* dst;  // out of the line + k1
   uint32_t N1;
-  float sc;
-  bool inv, ok;
-  FFT_D void operator()(uint32_t pos, c32 v) const {
-    if (ok) {
-      v.re *= sc;
-      v.im = inv ? -v.im * sc : v.im * sc;
-      dst[(uint64_t)N1 * pos] = v;
+  float sc, sci;  // scale of the real and imaginary parts (sci = -sc for inverse)
+  bool ok;
+  template <int R>
+  FFT_D void store(uint32_t o, uint32_t Ns, const c32* v) const {
+    if (!ok) return;
+    c32* dp = dst + (uint64_t)N1 * o;
+    const uint64_t step = (uint64_t)N1 * Ns;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      *dp = c32{v[r].re * sc, v[r].im * sci};
+      dp += step;
     }
   }
 };
@@ -196,8 +207,7 @@ FFT_D void ilv_stage(const c32* __restrict__ src, c32* __restrict__ dst, const S
     dft<float, R>(v);
     const uint32_t o = (j - k) * R + k;
     if (Epi::active && to_epi) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) epi(o + r * Ns, v[r]);
+      epi.template store<R>(o, Ns, v);
     } else {
       c32* db = dst + o * P + l;
 #pragma unroll
@@ -282,7 +292,7 @@ struct ChirpWalk {
 };
 
 FFT_D void copy_async(c32* dst, const c32* src, uint32_t n, uint32_t tid) {
-  for (uint32_t e = tid; e < n; e += kLongThreads) cp_async8_zfill(dst + e, src + e, true);
+  for (uint32_t e = tid; e < n; e += kLongThreads) cp_async8(dst + e, src + e);
 }
 
 // Issues the copies of one task into the landing buffer X (zero-filled
@@ -306,36 +316,52 @@ FFT_D void long_issue(const LongParams& p, const LongLenDesc& d, const LongTask&
     }
   }
   if (colk) {
-    // columns g0..g0+G-1: row n1 is the segment src[N2 n1 + g0 + l]
+    // columns g0..g0+G-1: row n1 is the segment src[N2 n1 + g0 + l]; rows
+    // n1 < nv of column c hold data (N2 n1 + c < lim), the rest are zeros
+    // (columns past N2, the zero-padded half of a chirped column) written
+    // directly: this buffer's previous task finished before the barrier
     const uint32_t lg = d.lgc, G = 1u << lg, P = G + 1;
     const uint32_t l = tid & (G - 1), S = kLongThreads >> lg;
     const uint32_t N2 = d.N2, Nx = d.N1;
-    const bool col_ok = g0 + l < N2;
+    const uint32_t c = g0 + l;
     const c32* src = (kind == LP_BCOL3) ? p.scratch + ln.scratch : p.in + ln.base;
     const uint32_t lim = (kind == LP_BCOL1) ? d.N : d.M;  // chirped pass: zero beyond the line
+    const uint32_t nv = c < N2 ? min(Nx, (lim - c + N2 - 1) / N2) : 0u;
     uint32_t i = tid >> lg;
-    uint32_t n = N2 * i + g0 + l;
     c32* dp = X + i * P + l;
+    const c32* sp = src + ((uint64_t)N2 * i + c);
+    const uint64_t sstep = (uint64_t)S * N2;
 #pragma unroll 4
+    for (; i < nv; i += S) {
+      cp_async8(dp, sp);
+      sp += sstep;
+      dp += S * P;
+    }
     for (; i < Nx; i += S) {
-      const bool ok = col_ok && n < lim;
-      cp_async8_zfill(dp, ok ? src + n : src, ok);
-      n += S * N2;
+      *dp = czero<float>();
       dp += S * P;
     }
   } else {
     // rows g0..g0+G-1 of the scratch: kLongThreads / G threads per row
-    // (a half-warp, a warp or two), each a run of consecutive values
+    // (a half-warp, a warp or two), each a run of consecutive values;
+    // rows past N1 are zeros
     const uint32_t lg = d.lgr, P = (1u << lg) + 1;
     const uint32_t N2 = d.N2, N1 = d.N1;
     const uint32_t tpr = kLongThreads >> lg, r = tid >> (kLongThreadsLog2 - lg), lane = tid & (tpr - 1);
-    const bool ok = g0 + r < N1;
-    const c32* row = p.scratch + ln.scratch + (uint64_t)(ok ? g0 + r : 0) * N2;
     c32* dp = X + lane * P + r;
+    if (g0 + r < N1) {
+      const c32* sp = p.scratch + ln.scratch + (uint64_t)(g0 + r) * N2 + lane;
 #pragma unroll 4
-    for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
-      cp_async8_zfill(dp, row + n2, ok);
-      dp += tpr * P;
+      for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
+        cp_async8(dp, sp);
+        sp += tpr;
+        dp += tpr * P;
+      }
+    } else {
+      for (uint32_t n2 = lane; n2 < N2; n2 += tpr) {
+        *dp = czero<float>();
+        dp += tpr * P;
+      }
     }
   }
 }
@@ -393,7 +419,7 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
     e.dst = p.out + ln.obase + (e.ok ? g0 + l : 0);
     e.N1 = N1;
     e.sc = d.scale;
-    e.inv = inv;
+    e.sci = inv ? -d.scale : d.scale;
     ilv_fft(X, W, sch, lg, tid, T, e);
     return;
   }
@@ -519,8 +545,8 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
   auto fetch_task = [&](uint32_t k) {
     const uint32_t t = task_of(k);
     if (t != kNone && tid < 4)
-      cp_async8_zfill(reinterpret_cast<uint64_t*>(&s_task[k & 3]) + tid,
-                      reinterpret_cast<const uint64_t*>(p.tasks + t) + tid, true);
+      cp_async8(reinterpret_cast<uint64_t*>(&s_task[k & 3]) + tid,
+                reinterpret_cast<const uint64_t*>(p.tasks + t) + tid);
   };
   // length descriptor of task k (whose record has landed) into s_len[k % 3],
   // unless that slot holds it already
@@ -535,7 +561,7 @@ __global__ void __launch_bounds__(kLongThreads, 2) k_long_pass(const __grid_cons
     const uint64_t* src = reinterpret_cast<const uint64_t*>(p.lens + len);
     uint64_t* dst = reinterpret_cast<uint64_t*>(&s_len[r]);
     for (uint32_t i = tid; i < sizeof(LongLenDesc) / 8; i += kLongThreads)
-      cp_async8_zfill(dst + i, src + i, true);
+      cp_async8(dst + i, src + i);
   };
   // data of task k (whose record and descriptor have landed) into landing
   // buffer k % 2, with its length's tables when that buffer's differ

@@ -17,7 +17,11 @@
 //   - resident plans are keyed by configuration without the batch and by a
 //     power-of-two batch bucket: a group's batch B runs as the binary
 //     decomposition of B over at most 13 cached plans, so no group size
-//     builds a new plan once its buckets exist.  Plans count against the
+//     builds a new plan once its buckets exist; a (configuration, batch)
+//     seen a second time gets a plan of exactly that batch and runs as one
+//     execution (recurring request shapes pay one plan build, not a
+//     decomposition per request).  A group of one 1D complex f32 request
+//     runs on a plan, not the line launch.  Plans count against the
 //     HBM budget and the least recently used ones are evicted (after their
 //     last execution has completed) when admission needs the room;
 //   - admission: a group is admitted when its device bytes (staging, the
@@ -134,6 +138,10 @@ struct Server {
   std::vector<double> lat;
   uint64_t completed = 0, failed = 0, groups = 0, line_groups = 0, coalesced = 0, transforms = 0;
   uint64_t evictions = 0;
+  // executions seen per exact (configuration, batch): a batch seen before
+  // runs on a plan of exactly that batch (one execution instead of the
+  // power-of-two decomposition); the map is reset when it grows large
+  std::unordered_map<std::string, uint32_t> seen_exact;
   double t_first = 0, t_last = 0;
   std::thread worker;
 
@@ -193,7 +201,7 @@ struct Server {
     return used + plan_bytes + registry_bytes() + need <= budget;
   }
 
-  // The resident plan of cfg (its batch already a bucket), created when new.
+  // The resident plan of cfg (a batch bucket or an exact batch), created when new.
   SPlan* get_plan(const Config& cfg, int32_t kind, b2f_status* st) {
     const std::string k = config_key(cfg, kind) + "|b" + std::to_string(cfg.batch);
     auto it = plans.find(k);
@@ -392,9 +400,17 @@ struct Server {
         const char* src = stage ? din : (const char*)r->in;
         char* dst = stage ? dout : (char*)r->out;
         uint64_t done_b = 0;
+        bool exact = false;
+        {
+          cfg.batch = left;
+          const std::string ek = config_key(cfg, r->kind) + "|b" + std::to_string(left);
+          if (seen_exact.size() > 65536) seen_exact.clear();
+          exact = plans.count(ek) > 0 || seen_exact[ek]++ > 0;
+        }
         while (left > 0 && st == B2F_OK) {
           uint64_t chunk = 1;
           while (chunk * 2 <= left && chunk * 2 <= 4096) chunk *= 2;
+          if (exact) chunk = left;
           cfg.batch = chunk;
           SPlan* sp = get_plan(cfg, r->kind, &st);
           if (!sp) break;
