@@ -458,8 +458,11 @@ struct Server {
     cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
     while (true) {
-      cv_work.wait_for(lk, std::chrono::microseconds(200),
-                       [&] { return stop || (!queue.empty() && !held) || !inflight.empty(); });
+      // wake for new work at once; with groups in flight, poll their
+      // completion every 20 us with the lock released (submitters and
+      // waiters get the lock meanwhile)
+      const auto poll = std::chrono::microseconds(inflight.empty() ? 2000 : 20);
+      cv_work.wait_for(lk, poll, [&] { return stop || (!queue.empty() && !held); });
       if (stop && queue.empty() && inflight.empty()) break;
       reap();
       // admit and group: the queue head's key, then every other queued
