@@ -124,7 +124,11 @@ b2f_status b2f_config_set_precision(b2f_config* cfg, int32_t precision);
  * optional ones), large_route (0 auto, 1 force-chunk, 2 force-four-step,
  * 3 force-segmented); and the B200 knobs lines_per_block (0 = planner's
  * choice), threads_per_block (0 = planner's choice), twiddle_table (1 =
- * stage twiddles from an FP64-built table, 0 = computed in-kernel). */
+ * stage twiddles from an FP64-built table, 0 = computed in-kernel),
+ * tensor_cores (1 = length-64 f32 lines on the tcgen05 layer) and
+ * radix_order (stage order of the shared-memory engine: 0 = the planner's,
+ * radix 16 first; 1 = reversed; nonzero keeps a line off the register
+ * kernel). */
 b2f_status b2f_config_set_tuning(b2f_config* cfg, const char* key, int64_t value);
 /* FftTuning::with_force_rader_axes / with_force_bluestein_axes
  * (src/tuning.rs:197-205): key "force_rader_axes" or "force_bluestein_axes". */
@@ -375,8 +379,8 @@ b2f_status b2f_df64_canary(int32_t device, uint32_t* words, uint64_t* exact_word
  * reference ancestors: FftTuning, src/tuning.rs:35-268, and the pipeline
  * cache snapshot, src/runtime/pipeline_cache.rs:14-395).  Creates the plan of
  * `cfg` (kind B2F_C2C/R2C/C2R) on `device`, times it and candidate tunings
- * of the kernel-shape knobs (twiddle_table, then lines_per_block 1..16, then
- * threads_per_block 64..512; `reps` executions each after two warm-ups, 0 =
+ * of the kernel-shape knobs (twiddle_table, then radix_order, then
+ * lines_per_block 1..16, then threads_per_block 64..512; `reps` executions each after two warm-ups, 0 =
  * 20) on buffers it allocates and fills with deterministic values, keeps the
  * fastest candidate whose output matches the default plan's within the
  * precision's tolerance (f32 2e-6, f64 1e-13, df64 1e-12 relative L2), and
@@ -388,10 +392,10 @@ b2f_status b2f_autotune(const b2f_config* cfg, int32_t kind, int32_t device, uin
 /* Records a tuning for cfg's key by hand (validated like a plan's tuning). */
 b2f_status b2f_tuning_snapshot_record(const b2f_config* cfg, int32_t kind, int64_t lines_per_block,
                                       int64_t threads_per_block, int64_t twiddle_table,
-                                      double best_us, double default_us);
+                                      int64_t radix_order, double best_us, double default_us);
 /* Copies the snapshot's tuning for cfg's key into cfg; *found = 0 or 1. */
 b2f_status b2f_tuning_snapshot_apply(b2f_config* cfg, int32_t kind, int32_t* found);
-/* The snapshot as versioned JSON (schema "wgpufft_b200.tuning", version 1,
+/* The snapshot as versioned JSON (schema "wgpufft_b200.tuning", version 2,
  * device, entries ordered by key, FNV-1a checksum over device and entries). */
 b2f_status b2f_tuning_snapshot_json(char* buf, uint64_t* len);
 b2f_status b2f_tuning_snapshot_save(const char* path);

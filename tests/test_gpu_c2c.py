@@ -164,6 +164,18 @@ def test_forced_routes_agree(cuda):
     assert O.rel_l2(a, ref) < 2e-6 and O.rel_l2(b, ref) < 2e-6
 
 
+@pytest.mark.parametrize("n", [360, 1000, 2048, 3003, 15015, 1009, 4099])
+@pytest.mark.parametrize("prec", [F32, F64])
+def test_reversed_radix_order(cuda, n, prec):
+    # tuning radix_order = 1 runs every stage schedule of the shared-memory
+    # engine in reverse (small odd radices first; power-of-two lines leave
+    # the register kernel): same transform within the tolerance
+    t = w.FftTuning().with_radix_order(1)
+    check_c2c(w.FftConfig.new(n).with_batch(3).with_precision(prec).with_tuning(t), seed=n)
+    check_c2c(w.FftConfig.new(n).with_direction(INV).with_precision(prec).with_tuning(t),
+              seed=n + 1)
+
+
 def test_computed_twiddles_match_table(cuda):
     x = signal(4 * 4096, 41)
     cfg = w.FftConfig.new(4096).with_batch(4)

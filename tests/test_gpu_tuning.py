@@ -35,8 +35,10 @@ def test_autotune_records_a_matching_fastest_candidate(cuda, cfg):
     tuned, found = w.tuned_config(cfg)
     assert found
     t = tuned.tuning()
-    assert (t.lines_per_block, t.threads_per_block, int(t.twiddle_table)) == \
-        (best["lines_per_block"], best["threads_per_block"], best["twiddle_table"])
+    assert (t.lines_per_block, t.threads_per_block, int(t.twiddle_table), t.radix_order) == \
+        (best["lines_per_block"], best["threads_per_block"], best["twiddle_table"],
+         best["radix_order"])
+    assert any(c["radix_order"] == 1 for c in rep["candidates"])
     check_c2c(tuned, seed=3)
 
 

@@ -23,14 +23,14 @@ def _seed():
     a = w.FftConfig.new(1024).with_batch(512)
     b = w.FftConfig.new_nd([64, 48])
     w.tuning_snapshot_record(a, K.C2c, 4, 256, 1, 10.5, 12.25)
-    w.tuning_snapshot_record(b, K.R2c, 2, 0, 0, 3.0, 3.5)
+    w.tuning_snapshot_record(b, K.R2c, 2, 0, 0, 3.0, 3.5, radix_order=1)
     return a, b
 
 
 def test_record_apply_and_canonical_json():
     a, b = _seed()
     snap = w.tuning_snapshot_json()
-    assert snap["schema"] == "wgpufft_b200.tuning" and snap["version"] == 1
+    assert snap["schema"] == "wgpufft_b200.tuning" and snap["version"] == 2
     keys = [e["key"] for e in snap["entries"]]
     assert keys == sorted(keys)
     assert "c2c/f32/forward/inverse/shape=1024/axes=0/batch=512" in keys
@@ -40,6 +40,7 @@ def test_record_apply_and_canonical_json():
     assert (tuned.tuning().lines_per_block, tuned.tuning().threads_per_block) == (4, 256)
     tuned_b, found_b = w.tuned_config(b, K.R2c)
     assert found_b and tuned_b.tuning().twiddle_table is False
+    assert tuned_b.tuning().radix_order == 1 and tuned.tuning().radix_order == 0
     # the key covers kind, shape, batch and precision
     assert not w.tuned_config(b, K.C2c)[1]
     assert not w.tuned_config(a.with_batch(511))[1]
@@ -64,6 +65,9 @@ def test_record_rejects_invalid_tuning():
     assert e.value.kind == "InvalidTuning"
     with pytest.raises(w.FftError):
         w.tuning_snapshot_record(c, K.C2c, 1, 64, 2)
+    with pytest.raises(w.FftError) as e:
+        w.tuning_snapshot_record(c, K.C2c, 1, 64, 1, radix_order=2)
+    assert e.value.kind == "InvalidTuning"
 
 
 def _load_bad(tmp_path, text, kind):
@@ -85,7 +89,7 @@ def test_load_rejections_keep_the_snapshot(tmp_path):
     _load_bad(tmp_path, json.dumps({**good, "extra": 1}), "SnapshotJson")
     _load_bad(tmp_path, json.dumps({**good, "schema": "wgpu-fft.pipeline-cache"}),
               "SnapshotSchemaMismatch")
-    _load_bad(tmp_path, json.dumps({**good, "version": 2}), "SnapshotVersionMismatch")
+    _load_bad(tmp_path, json.dumps({**good, "version": 1}), "SnapshotVersionMismatch")
     # an edited value: the checksum no longer matches
     edited = json.loads(json.dumps(good))
     edited["entries"][0]["lines_per_block"] = 8
@@ -107,5 +111,8 @@ def test_load_rejections_keep_the_snapshot(tmp_path):
     badval = json.loads(json.dumps(good))
     badval["entries"][0]["threads_per_block"] = 100
     _load_bad(tmp_path, json.dumps(badval), "SnapshotIntegrity")
+    badro = json.loads(json.dumps(good))
+    badro["entries"][0]["radix_order"] = 3
+    _load_bad(tmp_path, json.dumps(badro), "SnapshotIntegrity")
 
     assert w.tuning_snapshot_json() == before

@@ -70,7 +70,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "b2f_config_get_tuning": (st, [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
         "b2f_autotune": (st, [vp, i32, i32, u32, ctypes.c_char_p, ctypes.POINTER(u64)]),
         "b2f_tuning_snapshot_record": (st, [vp, i32, ctypes.c_int64, ctypes.c_int64,
-                                            ctypes.c_int64, ctypes.c_double, ctypes.c_double]),
+                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                            ctypes.c_double]),
         "b2f_tuning_snapshot_apply": (st, [vp, i32, ctypes.POINTER(i32)]),
         "b2f_tuning_snapshot_json": (st, [ctypes.c_char_p, ctypes.POINTER(u64)]),
         "b2f_tuning_snapshot_save": (st, [ctypes.c_char_p]),
@@ -194,7 +195,7 @@ _SCALAR_TUNING = (
     "large_route", "large_chunk_max_batches", "grouped_batch", "swap_to_2_stage_4_step",
     "swap_to_3_stage_4_step", "segmented_burst_depth", "max_storage_buffer_binding_size",
     "max_buffer_size", "fused_min_convolution_length", "fuse_long_axes", "fuse_small_volumes",
-    "lines_per_block", "threads_per_block", "twiddle_table", "tensor_cores",
+    "lines_per_block", "threads_per_block", "twiddle_table", "tensor_cores", "radix_order",
 )
 _TUNING_DEFAULTS = {
     "workgroup_size": 64, "fused_workgroup_size": 256, "rader_max_prime": 8192,
@@ -203,7 +204,7 @@ _TUNING_DEFAULTS = {
     "segmented_burst_depth": 2, "max_storage_buffer_binding_size": None,
     "max_buffer_size": None, "fused_min_convolution_length": 128, "fuse_long_axes": True,
     "fuse_small_volumes": True, "lines_per_block": 0, "threads_per_block": 0,
-    "twiddle_table": True, "tensor_cores": False,
+    "twiddle_table": True, "tensor_cores": False, "radix_order": 0,
 }
 
 
@@ -796,23 +797,24 @@ def tuned_config(config: FftConfig, kind: FftTransformKind = FftTransformKind.C2
         if not found.value:
             return config, False
         vals = {}
-        for k in ("lines_per_block", "threads_per_block", "twiddle_table"):
+        for k in ("lines_per_block", "threads_per_block", "twiddle_table", "radix_order"):
             v = ctypes.c_int64(0)
             _check(L.b2f_config_get_tuning(h.ptr, k.encode(), ctypes.byref(v)))
             vals[k] = int(v.value)
     t = config._tuning
     t = t.with_lines_per_block(vals["lines_per_block"]).with_threads_per_block(
-        vals["threads_per_block"]).with_twiddle_table(bool(vals["twiddle_table"]))
+        vals["threads_per_block"]).with_twiddle_table(bool(vals["twiddle_table"])).with_radix_order(
+        vals["radix_order"])
     return config.with_tuning(t), True
 
 
 def tuning_snapshot_record(config: FftConfig, kind: FftTransformKind, lines_per_block: int,
                            threads_per_block: int, twiddle_table: int, best_us: float = 0.0,
-                           default_us: float = 0.0) -> None:
+                           default_us: float = 0.0, radix_order: int = 0) -> None:
     with _ConfigHandle(config) as h:
         _check(lib().b2f_tuning_snapshot_record(h.ptr, int(kind), lines_per_block,
-                                                threads_per_block, twiddle_table, best_us,
-                                                default_us))
+                                                threads_per_block, twiddle_table, radix_order,
+                                                best_us, default_us))
 
 
 def tuning_snapshot_json() -> dict:

@@ -88,6 +88,7 @@ static int64_t* tuning_field(Tuning& t, const std::string& k) {
   if (k == "threads_per_block") return &t.threads_per_block;
   if (k == "twiddle_table") return &t.twiddle_table;
   if (k == "tensor_cores") return &t.tensor_cores;
+  if (k == "radix_order") return &t.radix_order;
   return nullptr;
 }
 

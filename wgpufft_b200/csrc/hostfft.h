@@ -69,4 +69,14 @@ void parallel_ranges(uint64_t n, F f) {
   for (auto& x : th) x.join();
 }
 
+// chirp_fwd(n, N) for n < N (the Bluestein pre- and post-multiplier), on
+// several host threads for long lines.
+inline std::vector<cd> chirp_table(uint64_t N) {
+  std::vector<cd> c(N);
+  parallel_ranges(N, [&](uint64_t a, uint64_t b) {
+    for (uint64_t n = a; n < b; ++n) c[n] = chirp_fwd(n, N);
+  });
+  return c;
+}
+
 }  // namespace b2f

@@ -71,6 +71,7 @@ struct BluesteinParams {
   uint32_t M;
   const void* bhat;  // FFT_M(b) / M, b = conjugate chirp, symmetric
   FastDiv dM, dMN;   // division by M and by M - N
+  const void* chirp;  // exp(-i pi n^2 / N) for n < N, FP64-built (null: computed in-kernel)
 };
 
 // Bluestein over a convolution too long for one CTA: the chirp
@@ -85,6 +86,7 @@ struct BlueElemParams {
   uint32_t N, M, mode, flags;
   uint64_t s, nlines;  // axis stride and number of lines (line l = o*s + i)
   double scale;
+  const void* chirp;   // exp(-i pi n^2 / N) for n < N, FP64-built (null: computed in-kernel)
 };
 
 // Generic real transforms (any N0): axis-0 lines expanded to full complex

@@ -205,6 +205,7 @@ __global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ Blues
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t N = p.N, M = bp.M, G = p.G, LD = p.LD;
   const Group g = group_of(p.io, G, blockIdx.x);
+  const C<S>* __restrict__ ctab = (const C<S>*)bp.chirp;
   {
     const C<S>* __restrict__ in = (const C<S>*)p.in;
     const bool conj_in = p.flags & PF_CONJ_IN;
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ Blues
       if (c < g.nvalid) {
         C<S> v = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
         if (conj_in) v.im = -v.im;
-        A[c * LD + pidx<PAD>(n)] = cmul(v, chirp<S>(n, N));
+        A[c * LD + pidx<PAD>(n)] = cmul(v, ctab ? ctab[n] : chirp<S>(n, N));
       }
     });
     const uint32_t pad = M - N;
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ Blues
     if (c < g.nvalid) {
       C<S> w = r2[c * LD + pidx<PAD>(k)];
       w.im = -w.im;
-      C<S> v = cmul(w, chirp<S>(k, N));
+      C<S> v = cmul(w, ctab ? ctab[k] : chirp<S>(k, N));
       if (fl & PF_SCALE) v = cscale(v, sc);
       if (fl & PF_CONJ_OUT) v.im = -v.im;
       out[g.out0 + (int64_t)c * g.dl_out + (int64_t)k * p.io.out_es] = v;
@@ -426,6 +427,7 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t N = p.N, M = p.M;
   const S sc = Scalar<S>::from_double(p.scale);
+  const C<S>* __restrict__ ctab = (const C<S>*)p.chirp;
   const uint32_t L = p.mode == BE_POST ? N : M;  // points per line this pass writes
   const uint64_t cpl = (L + kElemChunk - 1) / kElemChunk;
   for (uint64_t blk = blockIdx.x; blk < p.nlines * cpl; blk += gridDim.x) {
@@ -442,7 +444,7 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
         if (m < N) {
           v = in[base + (int64_t)m * (int64_t)p.s];
           if (p.flags & PF_CONJ_IN) v.im = -v.im;
-          v = cmul(v, chirp<S>(m, N));
+          v = cmul(v, ctab ? ctab[m] : chirp<S>(m, N));
         }
         ws[m] = v;
       }
@@ -460,7 +462,7 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
       for (uint32_t k = c0 + tid; k < c1; k += T) {
         C<S> w = ws[k];
         w.im = -w.im;
-        C<S> v = cmul(w, chirp<S>(k, N));
+        C<S> v = cmul(w, ctab ? ctab[k] : chirp<S>(k, N));
         if (p.flags & PF_SCALE) v = cscale(v, sc);
         if (p.flags & PF_CONJ_OUT) v.im = -v.im;
         out[base + (int64_t)k * (int64_t)p.s] = v;

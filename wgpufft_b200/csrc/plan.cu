@@ -244,6 +244,8 @@ static b2f_status validate_tuning(const Config& cfg) {
                           "must not exceed swap_to_3_stage_4_step when both thresholds are active");
   if (t.tensor_cores != 0 && t.tensor_cores != 1)
     return invalid_tuning("tensor_cores", t.tensor_cores, "InvalidValue", "must be 0 or 1");
+  if (t.radix_order != 0 && t.radix_order != 1)
+    return invalid_tuning("radix_order", t.radix_order, "InvalidValue", "must be 0 or 1");
   if (t.lines_per_block < 0)
     return invalid_tuning("lines_per_block", t.lines_per_block, "InvalidValue",
                           "must be zero (planner's choice) or positive");
@@ -410,6 +412,7 @@ struct Builder {
                      std::vector<cd>& tw) {
     radices = stage_radices(n);
     if (radices.empty() && n != 1) return false;
+    if (plan.cfg.tuning.radix_order == 1) std::reverse(radices.begin(), radices.end());
     if (radices.size() > FFT_MAX_STAGES) return false;
     std::memset(&sch, 0, sizeof(sch));
     sch.N = (uint32_t)n;
@@ -468,7 +471,8 @@ struct Builder {
 
   // Table pointers are patched after upload, by pass index and field.
   enum Field { F_LINES_TW, F_RADER_TW, F_BLUE_TW, F_REAL_TW, F_PERM_IN, F_PERM_OUT, F_RADER_BHAT,
-               F_BLUE_BHAT, F_BELEM_BHAT, F_TWS_A, F_TWS_B, F_SVOL_TW };
+               F_BLUE_BHAT, F_BELEM_BHAT, F_TWS_A, F_TWS_B, F_SVOL_TW, F_BLUE_CHIRP,
+               F_BELEM_CHIRP };
   struct Patch {
     size_t table, pass;
     Field field;
@@ -505,6 +509,8 @@ struct Builder {
         case F_TWS_A: ps.lines.tws_a = ptr; break;
         case F_TWS_B: ps.lines.tws_b = ptr; break;
         case F_SVOL_TW: ps.svol.tw = ptr; break;
+        case F_BLUE_CHIRP: ps.blue.chirp = ptr; break;
+        case F_BELEM_CHIRP: ps.belem.chirp = ptr; break;
       }
     }
   }
@@ -518,7 +524,11 @@ static bool try_pow2_pass(Builder& b, Pass& ps, uint64_t outer_n) {
   const uint64_t N = lp.N;
   const bool f32 = b.plan.prec == PREC_F32;
   if (N < 16 || (N & (N - 1)) || N > (f32 ? 8192u : 4096u)) return false;
-  if (b.plan.cfg.tuning.lines_per_block > 0 || b.plan.cfg.tuning.threads_per_block > 0) return false;
+  // the register kernel runs radix-16 stages then one smaller one: a
+  // reordered schedule or explicit launch shapes go to the shared-memory engine
+  if (b.plan.cfg.tuning.lines_per_block > 0 || b.plan.cfg.tuning.threads_per_block > 0 ||
+      b.plan.cfg.tuning.radix_order != 0)
+    return false;
   const LineIO& io = lp.io;
   bool colmajor;
   if (io.inner_n > 1 && io.in_inner == 1 && io.out_inner == 1) {
@@ -529,13 +539,17 @@ static bool try_pow2_pass(Builder& b, Pass& ps, uint64_t outer_n) {
   } else {
     return false;
   }
+  // f32 column tiles of 1024 points and more hold 32 values a thread (more
+  // adjacent columns per tile, longer row segments); every other line holds
+  // 16 (64 registers for f32: 4096- and 8192-point lines as 256 or 512
+  // threads, twice the resident warps of 32 values at 128 registers)
   int E = 16;
-  if (f32 && (N >= 4096 || (colmajor && N >= 1024))) E = 32;
-  // CTAs stay at 256 threads (up to about 128 registers a thread), so that
-  // two or more of them share an SM and one's loads overlap another's
-  // butterflies; column tiles of 8192-point lines keep 512 threads (two
-  // columns, 16-byte rows) rather than one 8-byte column
-  const uint32_t maxT = (colmajor && N > 4096) ? 512 : 256;
+  if (f32 && colmajor && N >= 1024) E = 32;
+  // CTAs stay at 256 threads, so that two or more of them share an SM and
+  // one's loads overlap another's butterflies; column tiles of 8192-point
+  // lines keep 512 threads (two columns, 16-byte rows) rather than one
+  // 8-byte column, and contiguous 8192-point f32 lines take 512 threads
+  const uint32_t maxT = ((colmajor && N > 4096) || (!colmajor && f32 && N == 8192)) ? 512 : 256;
   const uint32_t TL = (uint32_t)(N / E);
   if (TL == 0 || TL > maxT) return false;
   const uint32_t LD = (uint32_t)(N + (N >> 4) + 1);
@@ -694,6 +708,7 @@ static b2f_status add_bluestein_pass(Builder& b, int axis, uint64_t N, const Lin
   bp.dMN = make_fastdiv((uint32_t)(M - N));
   const std::vector<cd> bvec = chirp_spectrum(N, M);
   b.set_table(b.next_pass(), Builder::F_BLUE_BHAT, b.add_table(b.pack_complex(bvec)));
+  b.set_table(b.next_pass(), Builder::F_BLUE_CHIRP, b.add_table(b.pack_complex(chirp_table(N))));
   b.plan.passes.push_back(ps);
   return B2F_OK;
 }
@@ -742,7 +757,9 @@ static b2f_status add_bluestein_large(Builder& b, int axis, uint64_t N, uint64_t
   pre.label = "bluestein-forward-chirp-stage";
   pre.route = "bluestein";
   pre.belem = BlueElemParams{nullptr, nullptr, nullptr, (uint32_t)N, (uint32_t)M, BE_PRE,
-                             flags & PF_CONJ_IN, s, nlines, 1.0};
+                             flags & PF_CONJ_IN, s, nlines, 1.0, nullptr};
+  const size_t chirp_tab = b.add_table(b.pack_complex(chirp_table(N)));
+  b.set_table(b.next_pass(), Builder::F_BELEM_CHIRP, chirp_tab);
   b.plan.passes.push_back(pre);
   int cur = BUF_WS2;
   b2f_status st = add_complex_axis(b, axis, AxisKind::Mixed, M, 1, nlines, false, false, 1.0, &cur,
@@ -766,6 +783,7 @@ static b2f_status add_bluestein_large(Builder& b, int axis, uint64_t N, uint64_t
   post.belem.mode = BE_POST;
   post.belem.flags = flags & (PF_CONJ_OUT | PF_SCALE);
   post.belem.scale = scale;
+  b.set_table(b.next_pass(), Builder::F_BELEM_CHIRP, chirp_tab);
   b.plan.passes.push_back(post);
   return B2F_OK;
 }
@@ -1224,6 +1242,7 @@ static void build_diagnostics(Plan& plan) {
      << ",\"fuse_small_volumes\":" << (t.fuse_small_volumes ? "true" : "false")
      << ",\"lines_per_block\":" << t.lines_per_block << ",\"threads_per_block\":" << t.threads_per_block
      << ",\"twiddle_table\":" << (t.twiddle_table ? "true" : "false")
+     << ",\"radix_order\":" << t.radix_order
      << ",\"tensor_cores\":" << (t.tensor_cores ? "true" : "false") << "}";
   os << ",\"tuning\":{\"requested\":" << tj.str() << ",\"effective\":" << tj.str() << "}";
   os << ",\"supports_in_place\":" << (plan.in_place_kernels ? "true" : "false");

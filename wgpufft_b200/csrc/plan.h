@@ -38,6 +38,8 @@ struct Tuning {
   int64_t threads_per_block = 0;
   int64_t twiddle_table = 1;
   int64_t tensor_cores = 0;  // 1: length-64 f32 lines on the tcgen05 split-TF32 DFT layer
+  int64_t radix_order = 0;   // stage order of the shared-memory engine: 0 = planner's (radix 16
+                             // first, small odd radices last), 1 = reversed
 };
 
 struct Config {

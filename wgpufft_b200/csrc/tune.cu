@@ -2,8 +2,8 @@
 // b2f_tuning_snapshot_*).
 //
 // The autotuner times candidate FftTuning values of one configuration on the
-// device (the kernel-shape knobs this library honours: lines_per_block,
-// threads_per_block, twiddle_table), keeps the fastest candidate whose
+// device (the kernel-shape knobs this library honours: twiddle_table,
+// radix_order, lines_per_block, threads_per_block), keeps the fastest candidate whose
 // results match the default plan's within the precision's tolerance, and
 // records it in a process-wide snapshot keyed by the configuration (shape,
 // axes, batch, direction, normalisation, precision, transform kind).  The
@@ -30,10 +30,10 @@ namespace b2f {
 namespace {
 
 constexpr const char* kSchema = "wgpufft_b200.tuning";
-constexpr int64_t kVersion = 1;
+constexpr int64_t kVersion = 2;  // 2: entries carry radix_order
 
 struct Entry {
-  int64_t lines_per_block = 0, threads_per_block = 0, twiddle_table = 1;
+  int64_t lines_per_block = 0, threads_per_block = 0, twiddle_table = 1, radix_order = 0;
   double best_us = 0, default_us = 0;
 };
 
@@ -155,6 +155,7 @@ std::string entries_json(const std::map<std::string, Entry>& m) {
        << "\", \"lines_per_block\": " << kv.second.lines_per_block
        << ", \"threads_per_block\": " << kv.second.threads_per_block
        << ", \"twiddle_table\": " << kv.second.twiddle_table
+       << ", \"radix_order\": " << kv.second.radix_order
        << ", \"best_us\": " << fmt_double(kv.second.best_us)
        << ", \"default_us\": " << fmt_double(kv.second.default_us) << "}";
     first = false;
@@ -341,7 +342,8 @@ b2f_status parse_snapshot(const std::string& text, std::map<std::string, Entry>&
     Entry en;
     if (!as_int(e.get("lines_per_block"), en.lines_per_block) ||
         !as_int(e.get("threads_per_block"), en.threads_per_block) ||
-        !as_int(e.get("twiddle_table"), en.twiddle_table))
+        !as_int(e.get("twiddle_table"), en.twiddle_table) ||
+        !as_int(e.get("radix_order"), en.radix_order))
       return fail(B2F_ERR_SNAPSHOT_INTEGRITY,
                   "tuning snapshot integrity check failed: bad tuning values for " + key->str);
     const JVal* bu = e.get("best_us");
@@ -354,6 +356,7 @@ b2f_status parse_snapshot(const std::string& text, std::map<std::string, Entry>&
     c.tuning.lines_per_block = en.lines_per_block;
     c.tuning.threads_per_block = en.threads_per_block;
     c.tuning.twiddle_table = en.twiddle_table;
+    c.tuning.radix_order = en.radix_order;
     if (en.twiddle_table != 0 && en.twiddle_table != 1)
       return fail(B2F_ERR_SNAPSHOT_INTEGRITY,
                   "tuning snapshot integrity check failed: twiddle_table must be 0 or 1 for " + key->str);
@@ -430,7 +433,7 @@ double rel_l2(const std::vector<unsigned char>& a, const std::vector<unsigned ch
 }
 
 struct Candidate {
-  int64_t lpb, tpb, tt;
+  int64_t lpb, tpb, tt, ro;
   double us = -1;
   double err = 0;
   bool ok = false;
@@ -509,15 +512,17 @@ b2f_status autotune(const Config& base, int32_t kind, int device, uint32_t reps,
   const double tol = base.precision == B2F_F32 ? 2e-6 : (base.precision == B2F_F64 ? 1e-13 : 1e-12);
   std::vector<Candidate> tried;
   Candidate best{base.tuning.lines_per_block, base.tuning.threads_per_block,
-                 base.tuning.twiddle_table, default_us, 0.0, true, "default"};
-  auto run = [&](int64_t lpb, int64_t tpb, int64_t tt) {
+                 base.tuning.twiddle_table, base.tuning.radix_order, default_us, 0.0, true,
+                 "default"};
+  auto run = [&](int64_t lpb, int64_t tpb, int64_t tt, int64_t ro) {
     for (const auto& c : tried)
-      if (c.lpb == lpb && c.tpb == tpb && c.tt == tt) return;
-    Candidate c{lpb, tpb, tt};
+      if (c.lpb == lpb && c.tpb == tpb && c.tt == tt && c.ro == ro) return;
+    Candidate c{lpb, tpb, tt, ro};
     Config cfg = base;
     cfg.tuning.lines_per_block = lpb;
     cfg.tuning.threads_per_block = tpb;
     cfg.tuning.twiddle_table = tt;
+    cfg.tuning.radix_order = ro;
     Plan* pl = nullptr;
     if (create_plan(cfg, kind, device, &pl) != B2F_OK) {
       c.why = last_error();
@@ -536,12 +541,15 @@ b2f_status autotune(const Config& base, int32_t kind, int device, uint32_t reps,
     if (c.ok && c.us < best.us) best = c;
     tried.push_back(c);
   };
-  // staged search: twiddle source, then lines per block, then threads per block
-  for (int64_t tt : {1, 0}) run(0, 0, tt);
+  // staged search: twiddle source, then radix order, then lines per block,
+  // then threads per block
+  for (int64_t tt : {1, 0}) run(0, 0, tt, 0);
   const int64_t tt_best = best.tt;
-  for (int64_t lpb : {1, 2, 4, 8, 16}) run(lpb, 0, tt_best);
+  run(0, 0, tt_best, 1);
+  const int64_t ro_best = best.ro;
+  for (int64_t lpb : {1, 2, 4, 8, 16}) run(lpb, 0, tt_best, ro_best);
   const int64_t lpb_best = best.lpb;
-  for (int64_t tpb : {64, 128, 256, 512}) run(lpb_best, tpb, tt_best);
+  for (int64_t tpb : {64, 128, 256, 512}) run(lpb_best, tpb, tt_best, ro_best);
   cudaGetLastError();
   cleanup();
   const std::string key = config_key(base, kind);
@@ -554,6 +562,7 @@ b2f_status autotune(const Config& base, int32_t kind, int device, uint32_t reps,
     en.lines_per_block = best.lpb;
     en.threads_per_block = best.tpb;
     en.twiddle_table = best.tt;
+    en.radix_order = best.ro;
     en.best_us = best.us;
     en.default_us = default_us;
   }
@@ -561,11 +570,11 @@ b2f_status autotune(const Config& base, int32_t kind, int device, uint32_t reps,
   os << "{\"key\":\"" << json_escape(key) << "\",\"default_us\":" << fmt_double(default_us)
      << ",\"best_us\":" << fmt_double(best.us) << ",\"best\":{\"lines_per_block\":" << best.lpb
      << ",\"threads_per_block\":" << best.tpb << ",\"twiddle_table\":" << best.tt
-     << "},\"candidates\":[";
+     << ",\"radix_order\":" << best.ro << "},\"candidates\":[";
   for (size_t i = 0; i < tried.size(); ++i) {
     const Candidate& c = tried[i];
     os << (i ? "," : "") << "{\"lines_per_block\":" << c.lpb << ",\"threads_per_block\":" << c.tpb
-       << ",\"twiddle_table\":" << c.tt << ",\"us\":" << fmt_double(c.us) << ",\"rel_l2\":" << c.err
+       << ",\"twiddle_table\":" << c.tt << ",\"radix_order\":" << c.ro << ",\"us\":" << fmt_double(c.us) << ",\"rel_l2\":" << c.err
        << ",\"ok\":" << (c.ok ? "true" : "false") << ",\"note\":\"" << json_escape(c.why) << "\"}";
   }
   os << "]}";
@@ -603,13 +612,14 @@ b2f_status b2f_autotune(const b2f_config* cfg, int32_t kind, int32_t device, uin
 
 b2f_status b2f_tuning_snapshot_record(const b2f_config* cfg, int32_t kind, int64_t lines_per_block,
                                       int64_t threads_per_block, int64_t twiddle_table,
-                                      double best_us, double default_us) {
+                                      int64_t radix_order, double best_us, double default_us) {
   if (!cfg) return fail(B2F_ERR_INVALID_ARGUMENT, "null config");
   if (kind < B2F_C2C || kind > B2F_C2R) return fail(B2F_ERR_INVALID_ARGUMENT, "kind must be 0..=2");
   Config c = cfg->cfg;
   c.tuning.lines_per_block = lines_per_block;
   c.tuning.threads_per_block = threads_per_block;
   c.tuning.twiddle_table = twiddle_table;
+  c.tuning.radix_order = radix_order;
   if (twiddle_table != 0 && twiddle_table != 1)
     return fail(B2F_ERR_INVALID_TUNING, "InvalidTuning { field: twiddle_table }: must be 0 or 1");
   const b2f_status st = validate_config(c);
@@ -619,6 +629,7 @@ b2f_status b2f_tuning_snapshot_record(const b2f_config* cfg, int32_t kind, int64
   en.lines_per_block = lines_per_block;
   en.threads_per_block = threads_per_block;
   en.twiddle_table = twiddle_table;
+  en.radix_order = radix_order;
   en.best_us = best_us;
   en.default_us = default_us;
   return B2F_OK;
@@ -633,6 +644,7 @@ b2f_status b2f_tuning_snapshot_apply(b2f_config* cfg, int32_t kind, int32_t* fou
     cfg->cfg.tuning.lines_per_block = it->second.lines_per_block;
     cfg->cfg.tuning.threads_per_block = it->second.threads_per_block;
     cfg->cfg.tuning.twiddle_table = it->second.twiddle_table;
+    cfg->cfg.tuning.radix_order = it->second.radix_order;
   }
   return B2F_OK;
 }
