@@ -738,9 +738,29 @@ def main():
         c1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(world, c0.elapsed_time(c1)) / e2e_steps
+        # the PCIe bound beside it: the same bytes copied in and out
+        # concurrently (two streams, no transform), one whole-buffer copy each
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        cp0, cp1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        cp0.record(stream)
+        s_in.wait_event(cp0)
+        s_out.wait_event(cp0)
+        for _ in range(e2e_steps):
+            with torch.cuda.stream(s_in):
+                dx.copy_(hx, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                hy.copy_(dy, non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+        cp1.record(stream)
+        torch.cuda.synchronize()
+        copy_ms = cp0.elapsed_time(cp1) / e2e_steps
         e2e = {"value": len(all_lengths) / (e2e_ms / 1e3), "unit": "FFTs/s",
                "h2d_bytes_per_step": all_total * 8, "d2h_bytes_per_step": all_total * 8,
-               "ms_per_step": e2e_ms}
+               "ms_per_step": e2e_ms,
+               "copies_alone_ms_per_step": copy_ms,
+               "copies_alone_gbs_each_way": all_total * 8 / (copy_ms / 1e3) / 1e9}
 
     # ---- plain per-plan: one plan per length, one execute_checked per line,
     # all 20,000 executions recorded once into a CUDA graph (FftRecorder) and

@@ -163,7 +163,10 @@ def test_single_pass_and_four_step_stages():
     # p - 1 = 2*3*683 is not smooth: Bluestein over a 7-smooth length >= 2p-1
     assert d["stages"][0]["label"] == "bluestein-fused-workgroup-stage"
     m = d["stages"][0]["convolution_length"]
-    assert m >= 2 * 4099 - 1
+    assert 2 * 4099 - 1 <= m <= 9 * 4099 // 4
+    # chosen by estimated cost among the 7-smooth lengths that fit one CTA:
+    # 9216 = 2^10 * 3^2 (radix 16, 16, 4, 9) over 8232 = 2^3 * 3 * 7^3
+    assert m == 9216 and sorted(d["stages"][0]["radices"]) == [4, 9, 16, 16]
 
 
 def test_real_plans():

@@ -667,16 +667,55 @@ static b2f_status add_rader_pass(Builder& b, int axis, uint64_t p, const LineIO&
   return B2F_OK;
 }
 
-static uint64_t bluestein_length(uint64_t n) {
-  uint64_t m = 2 * n - 1;
-  while (!is_smooth7(m)) ++m;
-  return m;
+// Estimated instructions per point of one shared-memory engine stage of
+// radix R: about 10 for the shared-memory traffic, addressing and twiddle
+// product, plus the codelet's arithmetic.
+static double stage_cost(uint32_t R) {
+  switch (R) {
+    case 2: return 12.0;
+    case 3: case 4: return 14.0;
+    case 5: return 16.4;
+    case 7: return 20.3;
+    case 8: return 16.5;
+    case 9: return 18.9;
+    case 11: return 22.7;
+    case 13: return 23.8;
+    default: return 19.0;  // 16
+  }
+}
+
+// The Bluestein convolution length of a length-n line: the first 7-smooth
+// length >= 2n - 1, or, when that fits one CTA, the 7-smooth length up to
+// 2.25 n that also fits and has the lowest estimated cost (length x the
+// per-point cost of its stages): a few percent more points in radix-16/8
+// stages often beat the first length's radix-7 stages.  Multi-pass
+// convolutions (HBM-bound) keep the first length.
+static uint64_t bluestein_length(const Builder& b, uint64_t n) {
+  uint64_t m0 = 2 * n - 1;
+  while (!is_smooth7(m0)) ++m0;
+  if (!b.fits_one_cta(m0)) return m0;
+  auto cost = [](uint64_t m) {
+    double c = 0;
+    for (uint32_t R : stage_radices(m)) c += stage_cost(R);
+    return c * (double)m;
+  };
+  uint64_t best = m0;
+  double best_c = cost(m0);
+  for (uint64_t m = m0 + 1; m <= 9 * n / 4 && b.fits_one_cta(m); ++m) {
+    if (!is_smooth7(m)) continue;
+    const double c = cost(m);
+    if (c < best_c) {
+      best_c = c;
+      best = m;
+    }
+  }
+  return best;
 }
 
 static b2f_status add_bluestein_pass(Builder& b, int axis, uint64_t N, const LineIO& io,
                                      uint64_t outer_n, uint32_t flags, double scale, int src,
                                      int dst) {
-  const uint64_t M = bluestein_length(N);
+  const uint64_t M = bluestein_length(b, N);
   Pass ps;
   ps.kind = Pass::BLUESTEIN;
   ps.axis = axis;
@@ -745,7 +784,7 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
 // spectrum product, FFT_M again, chirp post-multiply into the output.
 static b2f_status add_bluestein_large(Builder& b, int axis, uint64_t N, uint64_t s, uint64_t O,
                                       uint32_t flags, double scale, int src, int dst) {
-  const uint64_t M = bluestein_length(N);
+  const uint64_t M = bluestein_length(b, N);
   const uint64_t nlines = s * O;
   b.need(BUF_WS2, nlines * M * b.cb());
   b.need(dst, N * s * O * b.cb());
@@ -846,7 +885,7 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
     kind = AxisKind::Bluestein;
   }
   if (kind == AxisKind::Bluestein) {
-    const uint64_t M = bluestein_length(N);
+    const uint64_t M = bluestein_length(b, N);
     b2f_status st;
     if (b.fits_one_cta(M))
       st = add_bluestein_pass(b, axis, N, io, outer_n, flags, scale, src, out_buf);
