@@ -551,9 +551,10 @@ def config_measurements(local, hbm_peak):
 
 
 def run_reference(args, world, rank):
-    """--impl reference: the reference's CPU path (the planned CPU port of
-    CpuFftPlan; the reference's Rust crate cannot be built here) on the host
-    cores, a bounded sample of the same workload per step."""
+    """--impl reference: the reference's CPU path on the host cores, all
+    threads: the faster of scipy.fft (pocketfft, the stand-in for the
+    crate's CpuFftPlan, whose rustfft backend cannot be built here) over
+    every line and the planned C port of CpuFftPlan over a bounded sample."""
     from wgpufft_b200 import workloads as W
     if rank != 0:
         return
@@ -597,6 +598,13 @@ def main():
                     help="use only the first K lines of the workload (profiling-sized cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        # the reference arm runs on rank 0's host cores alone; the other
+        # ranks exit at once, with no process group to wait on
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), 0)
+        return
     rep = dist_setup(args)
     world, rank, local = rep.world, rep.rank, rep.local
 
@@ -605,11 +613,6 @@ def main():
 
     def max_over_ranks(_world, value):
         return rep.max(value)
-
-    if args.impl == "reference":
-        run_reference(args, world, rank)
-        rep.close()
-        return
 
     import torch
     import wgpufft_b200 as w

@@ -71,9 +71,9 @@ cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, un
                         unsigned threads, size_t smem, cudaStream_t st) {
   switch (p) {
     case PREC_F32:
-      if (E == 32)
+      if (E == 32)  // column tiles only
         return colmajor ? launch_pow2_t<float, 32, true>(prm, grid, threads, smem, st)
-                        : launch_pow2_t<float, 32, false>(prm, grid, threads, smem, st);
+                        : cudaErrorInvalidValue;
       return colmajor ? launch_pow2_t<float, 16, true>(prm, grid, threads, smem, st)
                       : launch_pow2_t<float, 16, false>(prm, grid, threads, smem, st);
     case PREC_F64:

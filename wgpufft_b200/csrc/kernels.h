@@ -48,7 +48,8 @@ struct LinesParams {
   FastDiv d_tw;         // division by io.tw_div
   uint64_t tw_store_M;
   // PF_TW_STORE from tables (when tws_a is set): W_M^m = tws_a[m / L] *
-  // tws_b[m % L], L = d_tws.d, both tables built in FP64 and rounded once
+  // tws_b[m % L], L = d_tws.d (a power of two), both tables built in FP64
+  // and rounded once
   const void* tws_a;
   const void* tws_b;
   FastDiv d_tws;

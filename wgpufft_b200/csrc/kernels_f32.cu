@@ -18,7 +18,6 @@ template cudaError_t launch_c2r_t<float>(const RealParams&, unsigned, unsigned, 
 template cudaError_t launch_blue_elem_t<float>(const BlueElemParams&, cudaStream_t);
 template cudaError_t launch_pow2_t<float, 16, false>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_pow2_t<float, 16, true>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
-template cudaError_t launch_pow2_t<float, 32, false>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_pow2_t<float, 32, true>(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 template cudaError_t launch_real_elem_t<float>(const RealElemParams&, cudaStream_t);
 template cudaError_t launch_small_volume_t<float>(const SmallVolumeParams&, unsigned, size_t,

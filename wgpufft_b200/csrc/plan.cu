@@ -935,13 +935,14 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
     }
   }
   // W_M^{row * n} on the store of pass `idx` from two tables of about
-  // sqrt(M) values each
+  // sqrt(M) values each, split at a power of two L >= sqrt(M) (the
+  // exponent splits with a shift)
   auto store_twiddles = [&](size_t idx, uint64_t M) {
     LinesParams& lp = b.plan.passes[idx].lines;
     lp.tw_store_M = M;
     if (!b.plan.cfg.tuning.twiddle_table) return;
-    uint64_t L = (uint64_t)std::sqrt((double)M);
-    while (L * L < M) ++L;
+    uint64_t L = 1;
+    while (L * L < M) L <<= 1;
     std::vector<cd> ta, tb;
     for (uint64_t q = 0; q * L < M; ++q) ta.push_back(root_fwd(q * L, M));
     for (uint64_t q = 0; q < L; ++q) tb.push_back(root_fwd(q, M));
