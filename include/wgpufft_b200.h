@@ -128,7 +128,10 @@ b2f_status b2f_config_set_precision(b2f_config* cfg, int32_t precision);
  * tensor_cores (1 = length-64 f32 lines on the tcgen05 layer) and
  * radix_order (stage order of the shared-memory engine: 0 = the planner's,
  * radix 16 first; 1 = reversed; nonzero keeps a line off the register
- * kernel). */
+ * kernel) and tma_tiles (1 = f32 column-tile passes of <= 256 points staged
+ * through the Tensor Memory Accelerator in a persistent grid; 0, the
+ * default = plain loads, measured faster: these passes are bound by
+ * instruction issue, not by load latency). */
 b2f_status b2f_config_set_tuning(b2f_config* cfg, const char* key, int64_t value);
 /* FftTuning::with_force_rader_axes / with_force_bluestein_axes
  * (src/tuning.rs:197-205): key "force_rader_axes" or "force_bluestein_axes". */

@@ -5,7 +5,7 @@ ncu capture of a single kernel.
 
 python tests/profile_case.py --shape 1024 --batch 32768 [--iters 5]
        [--precision f32|f64|df64] [--inverse] [--kind c2c|r2c|c2r]
-       [--tensor-cores] [--in-place]
+       [--tensor-cores] [--tma] [--in-place]
 """
 from __future__ import annotations
 
@@ -28,6 +28,8 @@ def main() -> None:
     ap.add_argument("--in-place", action="store_true")
     ap.add_argument("--tensor-cores", action="store_true",
                     help="tuning tensor_cores = 1 (length-64 f32 lines on the tcgen05 layer)")
+    ap.add_argument("--tma", action="store_true",
+                    help="tuning tma_tiles = 1 (column tiles staged by TMA)")
     args = ap.parse_args()
     import torch
 
@@ -37,6 +39,8 @@ def main() -> None:
            .with_precision(prec[args.precision]))
     if args.tensor_cores:
         cfg = cfg.with_tuning(w.FftTuning().with_tensor_cores(True))
+    if args.tma:
+        cfg = cfg.with_tuning(cfg.tuning().with_tma_tiles(True))
     if args.inverse or args.kind == "c2r":
         cfg = cfg.with_direction(w.FftDirection.Inverse)
     plan = getattr(w.FftPlan, args.kind)(cfg, device=0)

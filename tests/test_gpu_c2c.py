@@ -9,7 +9,7 @@ import pytest
 
 import wgpufft_b200 as w
 from oracle import oracle as O
-from tests.gpu_util import TOL, check_c2c, from_device, run_c2c, signal, to_device
+from tests.gpu_util import TOL, check_c2c, from_device, oracle_c2c, run_c2c, signal, to_device
 
 pytestmark = pytest.mark.gpu
 
@@ -174,6 +174,25 @@ def test_reversed_radix_order(cuda, n, prec):
     check_c2c(w.FftConfig.new(n).with_batch(3).with_precision(prec).with_tuning(t), seed=n)
     check_c2c(w.FftConfig.new(n).with_direction(INV).with_precision(prec).with_tuning(t),
               seed=n + 1)
+
+
+@pytest.mark.parametrize("shape,batch", [([2048, 4096], 1), ([64, 256, 128], 2), ([1 << 16], 3),
+                                         ([100, 200], 2), ([256, 256, 256], 1)])
+def test_tma_column_tiles_equal_plain_loads(cuda, shape, batch):
+    # column passes of <= 256 points staged by TMA in a persistent grid give
+    # the same bits as the same passes with plain loads, and match the oracle
+    import torch
+    cfg = w.FftConfig.new_nd(shape).with_batch(batch)
+    x = signal(cfg.total_complex_len(), 11)
+    got, exact, plan = run_c2c(cfg.with_tuning(w.FftTuning().with_tma_tiles(True)), x)
+    stages = plan.diagnostics()["stages"]
+    if shape != [100, 200]:
+        assert any(s.get("tma_tiles") for s in stages), stages
+    off, _, plan_off = run_c2c(cfg.with_tuning(w.FftTuning().with_tma_tiles(False)), x)
+    assert not any(s.get("tma_tiles") for s in plan_off.diagnostics()["stages"])
+    assert np.array_equal(got, off)
+    assert O.rel_l2(got, oracle_c2c(cfg, exact)) <= 2e-6
+    plan.device_status()
 
 
 def test_computed_twiddles_match_table(cuda):

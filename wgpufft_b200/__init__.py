@@ -196,6 +196,7 @@ _SCALAR_TUNING = (
     "swap_to_3_stage_4_step", "segmented_burst_depth", "max_storage_buffer_binding_size",
     "max_buffer_size", "fused_min_convolution_length", "fuse_long_axes", "fuse_small_volumes",
     "lines_per_block", "threads_per_block", "twiddle_table", "tensor_cores", "radix_order",
+    "tma_tiles",
 )
 _TUNING_DEFAULTS = {
     "workgroup_size": 64, "fused_workgroup_size": 256, "rader_max_prime": 8192,
@@ -204,7 +205,7 @@ _TUNING_DEFAULTS = {
     "segmented_burst_depth": 2, "max_storage_buffer_binding_size": None,
     "max_buffer_size": None, "fused_min_convolution_length": 128, "fuse_long_axes": True,
     "fuse_small_volumes": True, "lines_per_block": 0, "threads_per_block": 0,
-    "twiddle_table": True, "tensor_cores": False, "radix_order": 0,
+    "twiddle_table": True, "tensor_cores": False, "radix_order": 0, "tma_tiles": False,
 }
 
 

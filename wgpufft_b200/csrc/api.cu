@@ -89,6 +89,7 @@ static int64_t* tuning_field(Tuning& t, const std::string& k) {
   if (k == "twiddle_table") return &t.twiddle_table;
   if (k == "tensor_cores") return &t.tensor_cores;
   if (k == "radix_order") return &t.radix_order;
+  if (k == "tma_tiles") return &t.tma_tiles;
   return nullptr;
 }
 
@@ -224,9 +225,9 @@ b2f_status b2f_plan_device_status(const b2f_plan* plan) {
   uint32_t flags = 0;
   cudaError_t e = cudaSuccess;
   for (const Pass& ps : p.passes) {
-    if (ps.kind != Pass::TC_DFT64) continue;
+    if (ps.kind != Pass::TC_DFT64 && !ps.tma) continue;
     uint32_t v = 0;
-    void* d = p.device_allocs[ps.tc_err];
+    void* d = p.device_allocs[ps.kind == Pass::TC_DFT64 ? ps.tc_err : ps.tma_err];
     e = cudaMemcpy(&v, d, sizeof(v), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && v) e = cudaMemset(d, 0, sizeof(v));
     if (e != cudaSuccess) break;
@@ -234,6 +235,8 @@ b2f_status b2f_plan_device_status(const b2f_plan* plan) {
   }
   if (prev >= 0 && prev != p.device) cudaSetDevice(prev);
   if (e != cudaSuccess) return fail(B2F_ERR_DEVICE, std::string("device status read failed: ") + cudaGetErrorString(e));
+  if (flags & 4)
+    return fail(B2F_ERR_DEVICE, "TMA column tiles: a bounded wait for a tile copy timed out");
   if (flags)
     return fail(B2F_ERR_DEVICE, std::string("tensor-core layer: a bounded wait for its matrix products timed out") +
                                     ((flags & 2) ? " (tensor memory freed with a product still pending)" : ""));

@@ -140,6 +140,13 @@ cudaError_t launch_lines(Prec p, const LinesParams& prm, unsigned grid, unsigned
                          size_t smem, cudaStream_t st);
 // Register-resident power-of-two lines: E values per thread, column-major
 // (adjacent lines first) or line-major thread order.
+// TMA-staged column tiles (tmatile.cu): whether a pass's shape can use
+// them, their CTAs per SM, and the launch (false: not launched, the input
+// view cannot be a tensor map; *err carries a launch error otherwise).
+bool tma_tile_shape_ok(const LinesParams& lp, uint64_t outer_n);
+int tma_tile_ctas_per_sm(const LinesParams& lp, unsigned threads);
+bool launch_pow2_tma(const LinesParams& lp, uint64_t ntiles, uint64_t outer_n, unsigned threads,
+                     unsigned grid, unsigned int* flag, cudaStream_t st, cudaError_t* err);
 cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
                         unsigned threads, size_t smem, cudaStream_t st);
 cudaError_t launch_rader(Prec p, const RaderParams& prm, unsigned grid, unsigned threads,

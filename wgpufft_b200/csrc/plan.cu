@@ -246,6 +246,8 @@ static b2f_status validate_tuning(const Config& cfg) {
     return invalid_tuning("tensor_cores", t.tensor_cores, "InvalidValue", "must be 0 or 1");
   if (t.radix_order != 0 && t.radix_order != 1)
     return invalid_tuning("radix_order", t.radix_order, "InvalidValue", "must be 0 or 1");
+  if (t.tma_tiles != 0 && t.tma_tiles != 1)
+    return invalid_tuning("tma_tiles", t.tma_tiles, "InvalidValue", "must be 0 or 1");
   if (t.lines_per_block < 0)
     return invalid_tuning("lines_per_block", t.lines_per_block, "InvalidValue",
                           "must be zero (planner's choice) or positive");
@@ -608,6 +610,21 @@ static b2f_status add_lines_pass(Builder& b, int axis, uint64_t N, const LineIO&
   }
   b.tw_table_for(lp.flags, tw, Builder::F_LINES_TW);
   Builder::fill_io_grid(lp, ps, outer_n);
+  // f32 column tiles of <= 256 points: staged by TMA into a persistent grid
+  // of as many CTAs as the SMs hold (needs a device to size the grid)
+  if (ps.kind == Pass::POW2 && ps.colmajor && ps.pow2_E == 16 && b.plan.prec == PREC_F32 &&
+      b.plan.cfg.tuning.tma_tiles && b.plan.device >= 0 && tma_tile_shape_ok(lp, outer_n)) {
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b.plan.device) == cudaSuccess) {
+      const int per_sm = tma_tile_ctas_per_sm(lp, ps.threads);
+      if (per_sm > 0 && nsm > 0) {
+        ps.tma = true;
+        ps.tma_grid = (unsigned)std::min<uint64_t>(ps.grid, (uint64_t)nsm * per_sm);
+        ps.tma_err = b.add_table(std::vector<unsigned char>(16, 0));
+      }
+    }
+    cudaGetLastError();
+  }
   b.plan.passes.push_back(ps);
   return B2F_OK;
 }
@@ -1259,6 +1276,7 @@ static void build_diagnostics(Plan& plan) {
        << ",\"smem_bytes\":" << p.smem << ",\"src\":" << p.src << ",\"dst\":" << p.dst;
     if (p.kind == Pass::BLUESTEIN) os << ",\"convolution_length\":" << p.blue.M;
     if (p.kind == Pass::RADER) os << ",\"convolution_length\":" << (p.rader.L.N - 1);
+    if (p.tma) os << ",\"tma_tiles\":true,\"persistent_grid\":" << p.tma_grid;
     os << "}";
   }
   os << "],\"buffer_requirements\":[";
@@ -1282,7 +1300,7 @@ static void build_diagnostics(Plan& plan) {
      << ",\"fuse_small_volumes\":" << (t.fuse_small_volumes ? "true" : "false")
      << ",\"lines_per_block\":" << t.lines_per_block << ",\"threads_per_block\":" << t.threads_per_block
      << ",\"twiddle_table\":" << (t.twiddle_table ? "true" : "false")
-     << ",\"radix_order\":" << t.radix_order
+     << ",\"radix_order\":" << t.radix_order << ",\"tma_tiles\":" << t.tma_tiles
      << ",\"tensor_cores\":" << (t.tensor_cores ? "true" : "false") << "}";
   os << ",\"tuning\":{\"requested\":" << tj.str() << ",\"effective\":" << tj.str() << "}";
   os << ",\"supports_in_place\":" << (plan.in_place_kernels ? "true" : "false");
@@ -1506,11 +1524,18 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
         p.lines.out = dst;
         e = launch_lines(plan.prec, p.lines, p.grid, p.threads, p.smem, st);
         break;
-      case Pass::POW2:
+      case Pass::POW2: {
         p.lines.in = src;
         p.lines.out = dst;
-        e = launch_pow2(plan.prec, p.pow2_E, p.colmajor, p.lines, p.grid, p.threads, p.smem, st);
+        bool done = false;
+        if (p.tma) {
+          const uint64_t outer = p.grid / ((uint64_t)p.lines.io.tiles * p.lines.io.mid_n);
+          done = launch_pow2_tma(p.lines, p.grid, outer, p.threads, p.tma_grid,
+                                 (unsigned int*)plan.device_allocs[p.tma_err], st, &e);
+        }
+        if (!done) e = launch_pow2(plan.prec, p.pow2_E, p.colmajor, p.lines, p.grid, p.threads, p.smem, st);
         break;
+      }
       case Pass::RADER:
         p.rader.L.in = src;
         p.rader.L.out = dst;

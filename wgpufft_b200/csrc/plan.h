@@ -40,6 +40,7 @@ struct Tuning {
   int64_t tensor_cores = 0;  // 1: length-64 f32 lines on the tcgen05 split-TF32 DFT layer
   int64_t radix_order = 0;   // stage order of the shared-memory engine: 0 = planner's (radix 16
                              // first, small odd radices last), 1 = reversed
+  int64_t tma_tiles = 0;     // 1: f32 column-tile passes of <= 256 points staged by TMA
 };
 
 struct Config {
@@ -89,6 +90,11 @@ struct Pass {
   float tc_scale = 1.0f;
   bool tc_inverse = false;
   size_t tc_table = 0, tc_err = 0;
+  // POW2 column tiles staged by TMA (tmatile.cu): persistent grid, the
+  // device_allocs index of the wait-timeout flag
+  bool tma = false;
+  unsigned tma_grid = 0;
+  size_t tma_err = 0;
 };
 
 struct Plan {
