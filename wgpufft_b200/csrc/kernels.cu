@@ -67,10 +67,38 @@ size_t max_smem_per_block() {
 template <class S, int E, bool COLMAJOR>
 cudaError_t launch_pow2_t(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 
+cudaError_t launch_pow2_fixed(int E, bool colmajor, const LinesParams& prm, unsigned grid,
+                              unsigned threads, size_t smem, cudaStream_t st);
+
+// The schedule the compile-time kernels assume for N = 2^m: radix-16
+// stages, then one radix 2^(m mod 4) stage, stage twiddle tables in order.
+static bool pow2_schedule_is_default(const LinesParams& prm) {
+  const uint32_t N = prm.N;
+  if (N < 16 || (N & (N - 1)) || prm.sch.N != N) return false;
+  const int lg = 31 - __builtin_clz(N);
+  const uint32_t nst = (uint32_t)(lg + 3) / 4;
+  if (prm.sch.nst != nst) return false;
+  uint32_t ns = 1, tw = 0;
+  for (uint32_t s = 0; s < nst; ++s) {
+    const uint32_t R = (int)s < lg / 4 ? 16u : (1u << (lg % 4));
+    const StageDesc& d = prm.sch.st[s];
+    if (d.R != R || d.Ns != ns || d.tw_off != tw) return false;
+    tw += ns * (R - 1);
+    ns *= R;
+  }
+  return true;
+}
+
 cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
                         unsigned threads, size_t smem, cudaStream_t st) {
   switch (p) {
     case PREC_F32:
+      // the compile-time kernel of this length when the schedule is the
+      // one it assumes; the generic one otherwise
+      if (pow2_schedule_is_default(prm)) {
+        const cudaError_t e = launch_pow2_fixed(E, colmajor, prm, grid, threads, smem, st);
+        if (e != cudaErrorInvalidValue) return e;
+      }
       if (E == 32)  // column tiles only
         return colmajor ? launch_pow2_t<float, 32, true>(prm, grid, threads, smem, st)
                         : cudaErrorInvalidValue;
