@@ -67,8 +67,8 @@ size_t max_smem_per_block() {
 template <class S, int E, bool COLMAJOR>
 cudaError_t launch_pow2_t(const LinesParams&, unsigned, unsigned, size_t, cudaStream_t);
 
-cudaError_t launch_pow2_fixed(int E, bool colmajor, const LinesParams& prm, unsigned grid,
-                              unsigned threads, size_t smem, cudaStream_t st);
+cudaError_t launch_pow2_fixed(Prec prec, int E, bool colmajor, const LinesParams& prm,
+                              unsigned grid, unsigned threads, size_t smem, cudaStream_t st);
 
 // The schedule the compile-time kernels assume for N = 2^m: radix-16
 // stages, then one radix 2^(m mod 4) stage, stage twiddle tables in order.
@@ -91,14 +91,14 @@ static bool pow2_schedule_is_default(const LinesParams& prm) {
 
 cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
                         unsigned threads, size_t smem, cudaStream_t st) {
+  // the compile-time kernel of this length (f32, f64) when the schedule is
+  // the one it assumes; the generic one otherwise
+  if ((p == PREC_F32 || p == PREC_F64) && pow2_schedule_is_default(prm)) {
+    const cudaError_t e = launch_pow2_fixed(p, E, colmajor, prm, grid, threads, smem, st);
+    if (e != cudaErrorInvalidValue) return e;
+  }
   switch (p) {
     case PREC_F32:
-      // the compile-time kernel of this length when the schedule is the
-      // one it assumes; the generic one otherwise
-      if (pow2_schedule_is_default(prm)) {
-        const cudaError_t e = launch_pow2_fixed(E, colmajor, prm, grid, threads, smem, st);
-        if (e != cudaErrorInvalidValue) return e;
-      }
       if (E == 32)  // column tiles only
         return colmajor ? launch_pow2_t<float, 32, true>(prm, grid, threads, smem, st)
                         : cudaErrorInvalidValue;

@@ -1,5 +1,5 @@
 // Register-resident power-of-two line kernel with the line length fixed at
-// compile time (f32, N = 2^LOGN, 16 <= N <= 8192).
+// compile time (f32 and f64, N = 2^LOGN, 16 <= N <= 8192).
 //
 // The same algorithm as k_pow2 (regfft.cuh): E values a thread in
 // registers, radix-16 stages then one radix 2, 4 or 8 stage, exchanges
@@ -8,14 +8,19 @@
 // of the schedule is a constant: the shared-memory exchanges and the
 // contiguous loads and stores address value q of a butterfly as a fixed
 // offset from one per-thread base (the pad of one slot per 16 values,
-// i + i/16, splits across the sum because every stride is a multiple of
-// 16), the twiddle offsets are constants, and the stage loop unrolls.  The
+// i + (i >> 4), splits across the sum because every stride is a multiple
+// of 16 and the first stage's bases are), the twiddle offsets are
+// constants, and the stage loop unrolls.  The
 // generic kernel recomputes those addresses per value from runtime strides
 // (about a third of its instructions are integer addressing).
 #pragma once
 #include "regfft.cuh"
 
 namespace b2f {
+
+// Pad shift of the power-of-two kernels' lines, every precision (the
+// planner sizes a line as LD = N + N/16 + 1, as for the generic kernel).
+constexpr int kPow2Pad = 4;
 
 template <int LOGN>
 struct P2Sched {
@@ -28,13 +33,15 @@ struct P2Sched {
   static constexpr int TW(int s) { return s == 0 ? 0 : TW(s - 1) + NS(s - 1) * (R(s - 1) - 1); }
 };
 
-// Slot of value i in a padded line (pidx<4>).
-FFT_HD constexpr uint32_t fx_pad(uint32_t i) { return i + (i >> 4); }
+// Offset of value b + x from the slot of b in a padded line (pidx<PAD>), for
+// x a multiple of 2^PAD or b a multiple of 2^PAD with x < 16.
+template <int PAD>
+FFT_HD constexpr uint32_t fx_off(uint32_t x) { return x + (x >> PAD); }
 
 // Stage s on the E register values: twiddles W_{NS R}^{q k} (k = j mod NS)
 // from the plan table or computed, then the radix-R codelet.
-template <int LOGN, int s, int E>
-FFT_D void fx_compute(cpx<float> (&v)[E], uint32_t t, const cpx<float>* __restrict__ tw) {
+template <class S, int LOGN, int s, int E>
+FFT_D void fx_compute(cpx<S> (&v)[E], uint32_t t, const cpx<S>* __restrict__ tw) {
   using P = P2Sched<LOGN>;
   constexpr int R = P::R(s), NS = P::NS(s), NB = E / R, TL = P::N / E;
   if constexpr (NS > 1) {
@@ -42,79 +49,83 @@ FFT_D void fx_compute(cpx<float> (&v)[E], uint32_t t, const cpx<float>* __restri
     for (int u = 0; u < NB; ++u) {
       const uint32_t k = (t + u * TL) & (NS - 1);
       if (tw != nullptr) {
-        const cpx<float>* tr = tw + P::TW(s) + k * (R - 1);
+        const cpx<S>* tr = tw + P::TW(s) + k * (R - 1);
 #pragma unroll
         for (int q = 1; q < R; ++q) v[u * R + q] = cmul(v[u * R + q], tr[q - 1]);
       } else {
-        apply_stage_twiddles<float, R>(v + u * R, k, NS * R);
+        apply_stage_twiddles<S, R>(v + u * R, k, NS * R);
       }
     }
   }
 #pragma unroll
-  for (int u = 0; u < NB; ++u) dft<float, R>(v + u * R);
+  for (int u = 0; u < NB; ++u) dft<S, R>(v + u * R);
 }
 
 // Stage s's outputs into the line's shared buffer: output o + r*NS of
 // butterfly j (o = (j - k) R + k).  NS is 1 (stage 0, R = 16: o is a
-// multiple of 16) or a multiple of 16, so pad(o + r NS) = pad(o) + r pad-stride.
-template <int LOGN, int s, int E>
-FFT_D void fx_write(const cpx<float> (&v)[E], cpx<float>* line, uint32_t t) {
+// multiple of 16) or a multiple of 16, so pad(o + r NS) = pad(o) + fx_off(r NS).
+template <class S, int LOGN, int s, int E>
+FFT_D void fx_write(const cpx<S> (&v)[E], cpx<S>* line, uint32_t t) {
   using P = P2Sched<LOGN>;
+  constexpr int PAD = kPow2Pad;
   constexpr int R = P::R(s), NS = P::NS(s), NB = E / R, TL = P::N / E;
-  constexpr uint32_t step = NS == 1 ? 1 : NS + NS / 16;
   static_assert(NS == 1 ? R == 16 : NS % 16 == 0, "separable padding");
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
     const uint32_t j = t + u * TL, k = j & (NS - 1);
-    cpx<float>* d = line + fx_pad((j - k) * R + k);
+    cpx<S>* d = line + pidx<PAD>((j - k) * R + k);
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[r * step] = v[u * R + r];
+    for (int r = 0; r < R; ++r) d[fx_off<PAD>(r * NS)] = v[u * R + r];
   }
 }
 
 // Stage s's inputs from the line's shared buffer: value j + q*NR, NR a
 // multiple of 16 for every stage after the first.
-template <int LOGN, int s, int E>
-FFT_D void fx_read(cpx<float> (&v)[E], const cpx<float>* line, uint32_t t) {
+template <class S, int LOGN, int s, int E>
+FFT_D void fx_read(cpx<S> (&v)[E], const cpx<S>* line, uint32_t t) {
   using P = P2Sched<LOGN>;
+  constexpr int PAD = kPow2Pad;
   constexpr int R = P::R(s), NR = P::NR(s), NB = E / R, TL = P::N / E;
   static_assert(NR % 16 == 0, "separable padding");
-  constexpr uint32_t step = NR + NR / 16;
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
-    const cpx<float>* b = line + fx_pad(t + u * TL);
+    const cpx<S>* b = line + pidx<PAD>(t + u * TL);
 #pragma unroll
-    for (int q = 0; q < R; ++q) v[u * R + q] = b[q * step];
+    for (int q = 0; q < R; ++q) v[u * R + q] = b[fx_off<PAD>(q * NR)];
   }
 }
 
 // Stages s.. of the line (barriers between the exchanges), then the
 // caller's store.
-template <int LOGN, int s, int E>
-FFT_D void fx_stages(cpx<float> (&v)[E], cpx<float>* line, uint32_t t,
-                     const cpx<float>* __restrict__ tw) {
+template <class S, int LOGN, int s, int E>
+FFT_D void fx_stages(cpx<S> (&v)[E], cpx<S>* line, uint32_t t, const cpx<S>* __restrict__ tw) {
   using P = P2Sched<LOGN>;
-  fx_compute<LOGN, s, E>(v, t, tw);
+  fx_compute<S, LOGN, s, E>(v, t, tw);
   if constexpr (s + 1 < P::NST) {
-    fx_write<LOGN, s, E>(v, line, t);
+    fx_write<S, LOGN, s, E>(v, line, t);
     __syncthreads();
-    fx_read<LOGN, s + 1, E>(v, line, t);
+    fx_read<S, LOGN, s + 1, E>(v, line, t);
     __syncthreads();
-    fx_stages<LOGN, s + 1, E>(v, line, t, tw);
+    fx_stages<S, LOGN, s + 1, E>(v, line, t, tw);
   }
 }
 
 // G lines of N = 2^LOGN points; blockDim = G * N / E (256 for 16-value
 // column tiles, up to 512 otherwise).  Shared memory: G * LD values,
-// LD = N + N/16 + 1.  Register budgets: 64 for contiguous lines (4 CTAs of
-// 256 threads per SM), 85 for 16-value column tiles (3 per SM), 128 for
-// 32-value ones.
-template <int E, bool COLMAJOR, int LOGN>
-__global__ void __launch_bounds__(COLMAJOR && E == 16 ? 256 : 512,
-                                  COLMAJOR ? (E == 16 ? 3 : 1) : 2)
+// LD = N + N/16 + 1.  f32 register budgets: 64 for contiguous lines (4
+// CTAs of 256 threads per SM), 85 for 16-value column tiles (3 per SM), 128
+// for 32-value ones; f64: 128 (256 threads, 2 per SM).
+template <class S, int E, bool COLMAJOR>
+struct FxBounds {
+  static constexpr int threads = sizeof(S) == 8 || (COLMAJOR && E == 16) ? 256 : 512;
+  static constexpr int blocks = sizeof(S) == 8 ? 2 : (COLMAJOR ? (E == 16 ? 3 : 1) : 2);
+};
+template <class S, int E, bool COLMAJOR, int LOGN>
+__global__ void __launch_bounds__(FxBounds<S, E, COLMAJOR>::threads, FxBounds<S, E, COLMAJOR>::blocks)
     k_pow2_fx(const __grid_constant__ LinesParams p) {
   using P = P2Sched<LOGN>;
-  using C = cpx<float>;
+  using C = cpx<S>;
+  constexpr int PAD = kPow2Pad;
   constexpr int N = P::N, TL = N / E, LAST = P::NST - 1;
   constexpr int R0 = P::R(0), NR0 = P::NR(0), RL = P::R(LAST), NSL = P::NS(LAST);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -149,11 +160,11 @@ __global__ void __launch_bounds__(COLMAJOR && E == 16 ? 256 : 512,
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = czero<float>();
+    for (int i = 0; i < E; ++i) v[i] = czero<S>();
   }
   C* line = sm + c * LD;
-  fx_stages<LOGN, 0, E>(v, line, t, tw);
-  const float sc = (float)p.scale;
+  fx_stages<S, LOGN, 0, E>(v, line, t, tw);
+  const S sc = Scalar<S>::from_double(p.scale);
   const uint32_t fl = p.flags;
   if (!(fl & PF_STORE_SMEM)) {
     // last stage: output n = j + r*NSL (j < NSL) straight to HBM
@@ -163,16 +174,27 @@ __global__ void __launch_bounds__(COLMAJOR && E == 16 ? 256 : 512,
     const uint64_t row = (fl & PF_TW_STORE) ? fdiv((uint32_t)(g.c0 + c), p.d_tw) : 0;
     const C* __restrict__ ta = (const C*)p.tws_a;
     const C* __restrict__ tb = (const C*)p.tws_b;
+    // twiddle W_M^{row n} (row n < M): from the power-of-two-split tables
+    // with a 32-bit exponent stepped by row * NSL per output when M < 2^32
+    const bool step_tw = ta != nullptr && p.d_tws.mul == 0 && p.tw_store_M <= 0xFFFFFFFFull;
+    const uint32_t sh = p.d_tws.shift, msk = (1u << sh) - 1;
 #pragma unroll
     for (int u = 0; u < E / RL; ++u) {
       const uint32_t j = t + u * TL;
       C* b = dst + (int64_t)j * es;
+      uint32_t m32 = (uint32_t)row * j;
+      const uint32_t dm = (uint32_t)row * NSL;
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
         C x = v[u * RL + r];
         if (fl & PF_TW_STORE) {
-          const uint64_t m = row * (uint64_t)(j + r * NSL);
-          x = cmul(x, ta ? tw_two_level(ta, tb, m, p.d_tws) : twiddle<float>(m % p.tw_store_M, p.tw_store_M));
+          if (step_tw) {
+            x = cmul(x, cmul(ta[m32 >> sh], tb[m32 & msk]));
+            m32 += dm;
+          } else {
+            const uint64_t m = row * (uint64_t)(j + r * NSL);
+            x = cmul(x, ta ? tw_two_level(ta, tb, m, p.d_tws) : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
+          }
         }
         if (fl & PF_SCALE) x = cscale(x, sc);
         if (fl & PF_CONJ_OUT) x.im = -x.im;
@@ -187,19 +209,19 @@ __global__ void __launch_bounds__(COLMAJOR && E == 16 ? 256 : 512,
   for (int u = 0; u < E / RL; ++u) {
     const uint32_t j = t + u * TL;
 #pragma unroll
-    for (int r = 0; r < RL; ++r) line[fx_pad(j + r * NSL)] = v[u * RL + r];
+    for (int r = 0; r < RL; ++r) line[pidx<PAD>(j + r * NSL)] = v[u * RL + r];
   }
   __syncthreads();
   C* __restrict__ out = (C*)p.out;
   const uint32_t T = blockDim.x;
   for_each_elem(N, p.dN, G, p.dG, true, tid, T, [&](uint32_t cc, uint32_t n) {
     if (cc < g.nvalid) {
-      C x = sm[cc * LD + fx_pad(n)];
+      C x = sm[cc * LD + pidx<PAD>(n)];
       if (fl & PF_TW_STORE) {
         const uint64_t row = fdiv((uint32_t)(g.c0 + cc), p.d_tw);
         const uint64_t m = row * (uint64_t)n;
         x = cmul(x, p.tws_a ? tw_two_level((const C*)p.tws_a, (const C*)p.tws_b, m, p.d_tws)
-                            : twiddle<float>(m % p.tw_store_M, p.tw_store_M));
+                            : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
       }
       if (fl & PF_SCALE) x = cscale(x, sc);
       if (fl & PF_CONJ_OUT) x.im = -x.im;
