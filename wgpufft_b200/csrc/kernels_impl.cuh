@@ -59,11 +59,32 @@ FFT_D void for_each_elem(uint32_t count, const FastDiv& dcount, uint32_t G, cons
   }
 }
 
+// Column tiles whose line count G is a power of two dividing the thread
+// count: each thread keeps one line c = tid mod G and walks its points
+// n = tid / G, + T / G, ... (no division per value, stepped addresses).
+FFT_D bool fixed_line_walk(uint32_t G, uint32_t T) {
+  return (G & (G - 1)) == 0 && (T & (G - 1)) == 0;
+}
+
 template <class S>
 FFT_D void load_lines(C<S>* sm, const LinesParams& p, const Group& g, uint32_t tid, uint32_t T) {
   constexpr int PAD = PadOf<S>::value;
   const C<S>* __restrict__ in = (const C<S>*)p.in;
   const bool conj_in = p.flags & PF_CONJ_IN;
+  if ((p.flags & PF_CFIRST_LOAD) && fixed_line_walk(p.G, T)) {
+    const uint32_t lg = 31 - __clz(p.G), c = tid & (p.G - 1), dn = T >> lg;
+    if (c < g.nvalid) {
+      const int64_t es = p.io.in_es;
+      const C<S>* src = in + g.in0 + (int64_t)c * g.dl_in;
+      C<S>* line = sm + c * p.LD;
+      for (uint32_t n = tid >> lg; n < p.N; n += dn) {
+        C<S> v = src[(int64_t)n * es];
+        if (conj_in) v.im = -v.im;
+        line[pidx<PAD>(n)] = v;
+      }
+    }
+    return;
+  }
   for_each_elem(p.N, p.dN, p.G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T,
                 [&](uint32_t c, uint32_t n) {
                   if (c < g.nvalid) {
@@ -81,6 +102,39 @@ FFT_D void store_lines(const C<S>* sm, const LinesParams& p, const Group& g, uin
   C<S>* __restrict__ out = (C<S>*)p.out;
   const uint32_t fl = p.flags;
   const S sc = Scalar<S>::from_double(p.scale);
+  if ((fl & PF_CFIRST_STORE) && fixed_line_walk(p.G, T)) {
+    const uint32_t lg = 31 - __clz(p.G), c = tid & (p.G - 1), dn = T >> lg;
+    if (c >= g.nvalid) return;
+    const int64_t es = p.io.out_es;
+    C<S>* dst = out + g.out0 + (int64_t)c * g.dl_out;
+    const C<S>* line = sm + c * p.LD;
+    const C<S>* __restrict__ ta = (const C<S>*)p.tws_a;
+    const C<S>* __restrict__ tb = (const C<S>*)p.tws_b;
+    const uint64_t row = (fl & PF_TW_STORE) ? fdiv((uint32_t)(g.c0 + c), p.d_tw) : 0;
+    // W_M^{row n}: a 32-bit exponent stepped by row * dn through the
+    // power-of-two-split tables when M < 2^32
+    const bool step_tw = ta != nullptr && p.d_tws.mul == 0 && p.tw_store_M <= 0xFFFFFFFFull;
+    const uint32_t sh = p.d_tws.shift, msk = (1u << sh) - 1;
+    const uint32_t n0 = tid >> lg;
+    uint32_t m32 = (uint32_t)row * n0;
+    const uint32_t dm = (uint32_t)row * dn;
+    for (uint32_t n = n0; n < p.N; n += dn) {
+      C<S> v = line[pidx<PAD>(n)];
+      if (fl & PF_TW_STORE) {
+        if (step_tw) {
+          v = cmul(v, cmul(ta[m32 >> sh], tb[m32 & msk]));
+          m32 += dm;
+        } else {
+          const uint64_t m = row * (uint64_t)n;
+          v = cmul(v, ta ? tw_two_level(ta, tb, m, p.d_tws) : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
+        }
+      }
+      if (fl & PF_SCALE) v = cscale(v, sc);
+      if (fl & PF_CONJ_OUT) v.im = -v.im;
+      dst[(int64_t)n * es] = v;
+    }
+    return;
+  }
   for_each_elem(p.N, p.dN, p.G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t n) {
     if (c < g.nvalid) {
       C<S> v = sm[c * p.LD + pidx<PAD>(n)];
