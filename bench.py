@@ -287,6 +287,11 @@ def serving_measurement(local, count=300, rates=(1e3, 1e4, 5e4, 1e5, 2e5),
         srv.hold(False)
         for r in warm:
             srv.wait(r, 600.0)
+        # and once back to back (the saturated case): the loop's streams,
+        # pool and coalesced groups reach their steady state
+        warm = [srv.submit_device(c, k, a, b) for c, k, a, b in zip(cfgs, kinds, ins, outs)]
+        for r in warm:
+            srv.wait(r, 600.0)
         per_rate = []
         for rate in rates:
             rng = np.random.default_rng(seed + 1)

@@ -301,7 +301,9 @@ b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_
  * results are written back to host_out) or device buffers
  * (b2f_server_submit_device).  When a group fails, no copy touching a
  * request's memory is pending by the time its wait returns the error.
- * hbm_budget_bytes 0 = 120 GB. */
+ * hbm_budget_bytes 0 = 120 GB.  The server raises the release threshold of
+ * the device's default memory pool to its budget (never lowers it), so the
+ * groups' stream-ordered allocations stay mapped across synchronisations. */
 typedef struct b2f_server b2f_server;
 b2f_status b2f_server_new(b2f_server** out, int32_t device, uint64_t hbm_budget_bytes,
                           int32_t nstreams, int32_t coalesce);

@@ -114,6 +114,7 @@ struct RealParams {
   double scale;
   FastDiv dh, dG, dN0, dP;  // h, G, N0, packed length
   Schedule sch;             // schedule of h (even N0) or N0 (odd N0)
+  const void* rtw;          // fixed-length kernels: W_N0^k for k < h (FP64-built)
 };
 
 // Small volumes (the crate's SmallVolumePlan, src/runtime/small_volume.rs:
@@ -147,6 +148,11 @@ bool tma_tile_shape_ok(const LinesParams& lp, uint64_t outer_n);
 int tma_tile_ctas_per_sm(const LinesParams& lp, unsigned threads);
 bool launch_pow2_tma(const LinesParams& lp, uint64_t ntiles, uint64_t outer_n, unsigned threads,
                      unsigned grid, unsigned int* flag, cudaStream_t st, cudaError_t* err);
+// Even-length real transforms whose half is a power of two (16..4096),
+// f32/f64, on the fixed-length register kernels (regfft_fixed.cuh):
+// cudaErrorInvalidValue when no such kernel exists.
+cudaError_t launch_real_fixed(Prec p, bool r2c, const RealParams& prm, unsigned grid,
+                              unsigned threads, size_t smem, cudaStream_t st);
 cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
                         unsigned threads, size_t smem, cudaStream_t st);
 cudaError_t launch_rader(Prec p, const RaderParams& prm, unsigned grid, unsigned threads,

@@ -79,3 +79,45 @@ cudaError_t launch_pow2_fixed(Prec prec, int E, bool colmajor, const LinesParams
 }
 
 }  // namespace b2f
+
+namespace b2f {
+
+template <class S, bool R2C, int LOGH>
+static cudaError_t fx_real(const RealParams& prm, unsigned grid, unsigned threads, size_t smem,
+                           cudaStream_t st) {
+  if (R2C) return launch(k_r2c_fx<S, LOGH>, prm, grid, threads, smem, st);
+  return launch(k_c2r_fx<S, LOGH>, prm, grid, threads, smem, st);
+}
+
+template <class S, bool R2C>
+static cudaError_t fx_real_any(int lg, const RealParams& prm, unsigned grid, unsigned threads,
+                               size_t smem, cudaStream_t st) {
+  switch (lg) {
+    case 4: return fx_real<S, R2C, 4>(prm, grid, threads, smem, st);
+    case 5: return fx_real<S, R2C, 5>(prm, grid, threads, smem, st);
+    case 6: return fx_real<S, R2C, 6>(prm, grid, threads, smem, st);
+    case 7: return fx_real<S, R2C, 7>(prm, grid, threads, smem, st);
+    case 8: return fx_real<S, R2C, 8>(prm, grid, threads, smem, st);
+    case 9: return fx_real<S, R2C, 9>(prm, grid, threads, smem, st);
+    case 10: return fx_real<S, R2C, 10>(prm, grid, threads, smem, st);
+    case 11: return fx_real<S, R2C, 11>(prm, grid, threads, smem, st);
+    case 12: return fx_real<S, R2C, 12>(prm, grid, threads, smem, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_real_fixed(Prec p, bool r2c, const RealParams& prm, unsigned grid,
+                              unsigned threads, size_t smem, cudaStream_t st) {
+  const uint32_t h = prm.h;
+  if (prm.N0 != 2 * h || h < 16 || h > 4096 || (h & (h - 1))) return cudaErrorInvalidValue;
+  const int lg = 31 - __builtin_clz(h);
+  if (p == PREC_F32)
+    return r2c ? fx_real_any<float, true>(lg, prm, grid, threads, smem, st)
+               : fx_real_any<float, false>(lg, prm, grid, threads, smem, st);
+  if (p == PREC_F64)
+    return r2c ? fx_real_any<double, true>(lg, prm, grid, threads, smem, st)
+               : fx_real_any<double, false>(lg, prm, grid, threads, smem, st);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace b2f

@@ -474,7 +474,7 @@ struct Builder {
   // Table pointers are patched after upload, by pass index and field.
   enum Field { F_LINES_TW, F_RADER_TW, F_BLUE_TW, F_REAL_TW, F_PERM_IN, F_PERM_OUT, F_RADER_BHAT,
                F_BLUE_BHAT, F_BELEM_BHAT, F_TWS_A, F_TWS_B, F_SVOL_TW, F_BLUE_CHIRP,
-               F_BELEM_CHIRP };
+               F_BELEM_CHIRP, F_REAL_RTW };
   struct Patch {
     size_t table, pass;
     Field field;
@@ -513,6 +513,7 @@ struct Builder {
         case F_SVOL_TW: ps.svol.tw = ptr; break;
         case F_BLUE_CHIRP: ps.blue.chirp = ptr; break;
         case F_BELEM_CHIRP: ps.belem.chirp = ptr; break;
+        case F_REAL_RTW: ps.real.rtw = ptr; break;
       }
     }
   }
@@ -1082,11 +1083,37 @@ static b2f_status add_real_pass(Builder& b, bool r2c, uint64_t N0, uint64_t nlin
                     " } (real axis-0 lines need an even length whose half is 13-smooth, or an odd 13-smooth length, within one CTA)");
   rp.LD = b.ld_for(nbuf);
   uint32_t G, T;
-  if (!b.choose_launch(nfft, 2 * (size_t)rp.LD * b.cb(), nlines, false, &G, &T))
-    return fail(B2F_ERR_UNSUPPORTED_LENGTH, "real line does not fit a CTA");
+  const Tuning& tn = b.plan.cfg.tuning;
+  const uint64_t h = N0 / 2;
+  // even N0 with a power-of-two half of 16..4096 (f32, f64; the planner's
+  // stage order, no explicit launch shape): the fixed-length register
+  // kernels, h/16 threads a line, one buffer of LD = h + h/16 + 1 per line
+  ps.real_fx = even && h >= 16 && h <= 4096 && (h & (h - 1)) == 0 &&
+               (b.plan.prec == PREC_F32 || b.plan.prec == PREC_F64) && tn.radix_order == 0 &&
+               tn.lines_per_block <= 0 && tn.threads_per_block <= 0;
+  if (ps.real_fx) {
+    const uint64_t TL = h / 16;
+    rp.LD = (uint32_t)(h + h / 16 + 1);
+    uint64_t g = std::max<uint64_t>(1, 256 / TL);
+    g = std::min<uint64_t>(g, std::max<uint64_t>(nlines, 1));
+    while (g > 1 && g * rp.LD * b.cb() > b.smem_budget) g >>= 1;
+    if (g * rp.LD * b.cb() > b.smem_budget) ps.real_fx = false;
+    G = (uint32_t)g;
+    T = (uint32_t)(g * TL);
+  }
+  if (!ps.real_fx) {
+    rp.LD = b.ld_for(nbuf);
+    if (!b.choose_launch(nfft, 2 * (size_t)rp.LD * b.cb(), nlines, false, &G, &T))
+      return fail(B2F_ERR_UNSUPPORTED_LENGTH, "real line does not fit a CTA");
+  }
   rp.G = G;
   ps.threads = T;
-  ps.smem = 2 * (size_t)G * rp.LD * b.cb();
+  ps.smem = (ps.real_fx ? 1 : 2) * (size_t)G * rp.LD * b.cb();
+  if (ps.real_fx) {
+    std::vector<cd> rt(h);
+    for (uint64_t k = 0; k < h; ++k) rt[k] = root_fwd(k, N0);
+    b.set_table(b.next_pass(), Builder::F_REAL_RTW, b.add_table(b.pack_complex(rt)));
+  }
   rp.dh = make_fastdiv(std::max<uint32_t>(rp.h, 1));
   rp.dG = make_fastdiv(G);
   rp.dN0 = make_fastdiv((uint32_t)N0);
@@ -1547,14 +1574,15 @@ static b2f_status run_passes(const Plan& plan, cudaStream_t st, const void* in, 
         e = launch_bluestein(plan.prec, p.blue, p.grid, p.threads, p.smem, st);
         break;
       case Pass::R2C:
-        p.real.in = src;
-        p.real.out = dst;
-        e = launch_r2c(plan.prec, p.real, p.grid, p.threads, p.smem, st);
-        break;
       case Pass::C2R:
         p.real.in = src;
         p.real.out = dst;
-        e = launch_c2r(plan.prec, p.real, p.grid, p.threads, p.smem, st);
+        if (p.real_fx)
+          e = launch_real_fixed(plan.prec, p.kind == Pass::R2C, p.real, p.grid, p.threads, p.smem, st);
+        else if (p.kind == Pass::R2C)
+          e = launch_r2c(plan.prec, p.real, p.grid, p.threads, p.smem, st);
+        else
+          e = launch_c2r(plan.prec, p.real, p.grid, p.threads, p.smem, st);
         break;
       case Pass::SCALE_COPY:
         e = launch_scale_copy(plan.prec, src, dst, p.copy_n, p.copy_scale, p.copy_conj, st);

@@ -90,6 +90,9 @@ struct Pass {
   float tc_scale = 1.0f;
   bool tc_inverse = false;
   size_t tc_table = 0, tc_err = 0;
+  // R2C / C2R on the fixed-length register kernels (even N0, h = N0/2 a
+  // power of two)
+  bool real_fx = false;
   // POW2 column tiles staged by TMA (tmatile.cu): persistent grid, the
   // device_allocs index of the wait-timeout flag
   bool tma = false;

@@ -231,3 +231,135 @@ __global__ void __launch_bounds__(FxBounds<S, E, COLMAJOR>::threads, FxBounds<S,
 }
 
 }  // namespace b2f
+
+namespace b2f {
+
+// Real transforms of even length N0 = 2h, h = 2^LOGH (16 <= h <= 4096),
+// lines contiguous: the h-point complex FFT of the packed pairs runs in the
+// fixed-length register kernel; G = blockDim / (h/16) lines per CTA, one
+// shared-memory buffer of G * LD values (exchanges and the pre/post
+// processing, which pairs k with h - k).  rtw: W_N0^k for k < h, built in
+// FP64 and rounded once.
+template <class S>
+struct FxRealBounds {
+  static constexpr int blocks = sizeof(S) == 8 ? 2 : 3;
+};
+
+// R2C: z[n] = x[2n] + i x[2n+1], Z = FFT_h(z), then for k <= h/2:
+// X[k] = E + W^k O and X[h-k] = conj(E - W^k O), E = (Z[k] + conj Z[h-k])/2,
+// O = -i (Z[k] - conj Z[h-k])/2, into the packed line of h + 1 values.
+template <class S, int LOGH>
+__global__ void __launch_bounds__(256, FxRealBounds<S>::blocks)
+    k_r2c_fx(const __grid_constant__ RealParams p) {
+  using P = P2Sched<LOGH>;
+  using C = cpx<S>;
+  constexpr int E = 16, PAD = kPow2Pad, H = P::N, TL = H / E, LAST = P::NST - 1;
+  constexpr int NR0 = P::NR(0), RL = P::R(LAST), NSL = P::NS(LAST);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  const uint32_t tid = threadIdx.x, G = p.G, LD = p.LD;
+  const uint32_t t = tid & (TL - 1), c = tid >> (31 - __clz(TL));
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const bool valid = l0 + c < p.nlines;
+  C v[E];
+  if (valid) {
+    const C* __restrict__ src = (const C*)p.in + (l0 + c) * H + t;
+#pragma unroll
+    for (int q = 0; q < E; ++q) v[q] = src[q * NR0];
+  } else {
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = czero<S>();
+  }
+  C* line = sm + c * LD;
+  fx_stages<S, LOGH, 0, E>(v, line, t, (p.flags & PF_TW_TABLE) ? (const C*)p.tw : nullptr);
+  // Z in natural order (the last exchange's reads ended with a barrier)
+#pragma unroll
+  for (int u = 0; u < E / RL; ++u) {
+    const uint32_t j = t + u * TL;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) line[pidx<PAD>(j + r * NSL)] = v[u * RL + r];
+  }
+  __syncthreads();
+  if (!valid) return;
+  const C* __restrict__ rtw = (const C*)p.rtw;
+  const S half = Scalar<S>::from_double(0.5);
+  const S sc = Scalar<S>::from_double(p.scale);
+  C* __restrict__ out = (C*)p.out + (l0 + c) * (H + 1);
+  for (uint32_t k = t; k <= H / 2; k += TL) {
+    const C a = line[pidx<PAD>(k)];
+    const C b = conj(line[pidx<PAD>(k == 0 ? 0 : H - k)]);
+    const C Ev = cscale(a + b, half);
+    const C Ov = cscale(mul_neg_i(a - b), half);
+    const C WO = cmul(Ov, rtw[k]);
+    C xk = Ev + WO;
+    C xh = conj(Ev - WO);
+    if (p.flags & PF_SCALE) {
+      xk = cscale(xk, sc);
+      xh = cscale(xh, sc);
+    }
+    out[k] = xk;
+    if (H - k != k) out[H - k] = xh;
+  }
+}
+
+// C2R: Z[n] = conj(P + i conj(W^n) Q), P = X[n] + conj X[h-n], Q = X[n] -
+// conj X[h-n] (imaginary parts of X[0] and X[h] ignored), for every n < h,
+// built straight into the first stage's registers; the forward FFT of the
+// conjugate, conjugated, gives (x[2n], x[2n+1]).
+template <class S, int LOGH>
+__global__ void __launch_bounds__(256, FxRealBounds<S>::blocks)
+    k_c2r_fx(const __grid_constant__ RealParams p) {
+  using P = P2Sched<LOGH>;
+  using C = cpx<S>;
+  constexpr int E = 16, PAD = kPow2Pad, H = P::N, TL = H / E, LAST = P::NST - 1;
+  constexpr int NR0 = P::NR(0), RL = P::R(LAST), NSL = P::NS(LAST);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  const uint32_t tid = threadIdx.x, G = p.G, LD = p.LD;
+  const uint32_t t = tid & (TL - 1), c = tid >> (31 - __clz(TL));
+  const uint64_t l0 = (uint64_t)blockIdx.x * G;
+  const bool valid = l0 + c < p.nlines;
+  C* line = sm + c * LD;
+  if (valid) {
+    const C* __restrict__ src = (const C*)p.in + (l0 + c) * (H + 1);
+    for (uint32_t k = t; k <= H; k += TL) line[pidx<PAD>(k)] = src[k];
+  }
+  __syncthreads();
+  const C* __restrict__ rtw = (const C*)p.rtw;
+  C v[E];
+  if (valid) {
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const uint32_t n = t + q * NR0;
+      C Xk = line[pidx<PAD>(n)];
+      C Xh = line[pidx<PAD>(H - n)];
+      if (n == 0) {
+        Xk.im = Scalar<S>::zero();
+        Xh.im = Scalar<S>::zero();
+      }
+      const C Pp = Xk + conj(Xh);
+      const C Q = Xk - conj(Xh);
+      v[q] = conj(Pp + mul_i(cmulc(Q, rtw[n])));
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = czero<S>();
+  }
+  __syncthreads();  // every X read before the exchanges reuse the buffer
+  fx_stages<S, LOGH, 0, E>(v, line, t, (p.flags & PF_TW_TABLE) ? (const C*)p.tw : nullptr);
+  if (!valid) return;
+  const S sc = Scalar<S>::from_double(p.scale);
+  C* __restrict__ out = (C*)p.out + (l0 + c) * H;
+#pragma unroll
+  for (int u = 0; u < E / RL; ++u) {
+    const uint32_t j = t + u * TL;
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      C x = conj(v[u * RL + r]);
+      if (p.flags & PF_SCALE) x = cscale(x, sc);
+      out[j + r * NSL] = x;
+    }
+  }
+}
+
+}  // namespace b2f

@@ -592,6 +592,19 @@ b2f_status b2f_server_new(b2f_server** out, int32_t device, uint64_t hbm_budget_
   s->budget = hbm_budget_bytes ? hbm_budget_bytes : (120ull << 30);
   s->nstreams = std::max(1, std::min(16, (int)nstreams));
   s->coalesce = coalesce != 0;
+  // the groups' stream-ordered allocations (staging, line task lists) come
+  // from the device's default pool: keep up to the budget mapped across
+  // synchronisations instead of returning it and mapping it anew per group
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (keep < s->budget) {
+      keep = s->budget;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
+  cudaGetLastError();
   for (int i = 0; i < s->nstreams; ++i) {
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
