@@ -37,6 +37,24 @@ def test_f32_bluestein_lengths(cuda, n):
     check_c2c(w.FftConfig.new(n).with_direction(INV), seed=n + 1)
 
 
+@pytest.mark.parametrize("n,prec,tuning", [
+    (40961, F32, w.FftTuning().with_force_rader_axes([0])),        # 2^13 * 5 + 1, forced
+    (7681, F64, None),                                             # too long for one CTA in f64
+    (7681, DF64, None),
+    (65537, F64, w.FftTuning().with_rader_max_prime(1 << 20)),     # 2^16 + 1
+])
+def test_multipass_rader(cuda, n, prec, tuning):
+    # primes whose line does not fit one CTA and whose p - 1 is smooth: the
+    # gather, FFT_{p-1}, spectrum product, FFT_{p-1}, scatter passes
+    cfg = w.FftConfig.new(n).with_batch(2).with_precision(prec)
+    if tuning is not None:
+        cfg = cfg.with_tuning(tuning)
+    check_c2c(cfg, seed=n)
+    check_c2c(cfg.with_direction(INV).with_normalization(w.Normalization.Orthogonal), seed=n + 1)
+    labels = [st["label"] for st in w.FftPlan.c2c(cfg).diagnostics()["stages"]]
+    assert labels[0] == "rader-gather-stage" and labels[-1] == "rader-scatter-stage", labels
+
+
 @pytest.mark.parametrize("n", [622423, 1268090])
 def test_f32_long_bluestein_lines(cuda, n):
     # one line whose Bluestein convolution spans many CTAs (prime; 2*5*173*733):

@@ -79,7 +79,11 @@ struct BluesteinParams {
 // pre-multiply (in layout -> workspace lines of M), the spectrum product
 // (in place on the workspace) and the chirp post-multiply (workspace ->
 // out layout) run as separate passes around multi-pass FFT_M.
-enum BlueElemMode : uint32_t { BE_PRE = 0, BE_MID = 1, BE_POST = 2 };
+// Elementwise passes of the multi-pass Bluestein (BE_PRE/MID/POST) and
+// Rader (BE_RADER_*) routes.
+enum BlueElemMode : uint32_t {
+  BE_PRE = 0, BE_MID = 1, BE_POST = 2, BE_RADER_PRE = 3, BE_RADER_MID = 4, BE_RADER_POST = 5
+};
 struct BlueElemParams {
   const void* in;
   void* out;
@@ -88,6 +92,11 @@ struct BlueElemParams {
   uint64_t s, nlines;  // axis stride and number of lines (line l = o*s + i)
   double scale;
   const void* chirp;   // exp(-i pi n^2 / N) for n < N, FP64-built (null: computed in-kernel)
+  // Rader (N = p prime, M = p - 1): perm_in[q] = g^q, perm_out[n-1] = r with
+  // g^-r = n, and two values a line (x[0], X[0]) kept between the passes
+  const uint32_t* perm_in;
+  const uint32_t* perm_out;
+  void* x0;
 };
 
 // Generic real transforms (any N0): axis-0 lines expanded to full complex

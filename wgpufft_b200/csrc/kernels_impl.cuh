@@ -482,7 +482,8 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
   const uint32_t N = p.N, M = p.M;
   const S sc = Scalar<S>::from_double(p.scale);
   const C<S>* __restrict__ ctab = (const C<S>*)p.chirp;
-  const uint32_t L = p.mode == BE_POST ? N : M;  // points per line this pass writes
+  // points per line this pass writes
+  const uint32_t L = (p.mode == BE_POST || p.mode == BE_RADER_POST) ? N : M;
   const uint64_t cpl = (L + kElemChunk - 1) / kElemChunk;
   for (uint64_t blk = blockIdx.x; blk < p.nlines * cpl; blk += gridDim.x) {
     const uint64_t l = blk / cpl;
@@ -509,6 +510,49 @@ __global__ void __launch_bounds__(256) k_blue_elem(const __grid_constant__ BlueE
         C<S> v = cmul(ws[k], bhat[k]);
         v.im = -v.im;
         ws[k] = v;
+      }
+    } else if (p.mode == BE_RADER_PRE) {
+      // a[q] = x[g^q] into the workspace line; x[0] kept
+      const C<S>* __restrict__ in = (const C<S>*)p.in;
+      C<S>* __restrict__ ws = (C<S>*)p.out + l * M;
+      for (uint32_t q = c0 + tid; q < c1; q += T) {
+        C<S> v = in[base + (int64_t)p.perm_in[q] * (int64_t)p.s];
+        if (p.flags & PF_CONJ_IN) v.im = -v.im;
+        ws[q] = v;
+      }
+      if (c0 == 0 && tid == 0) {
+        C<S> v = in[base];
+        if (p.flags & PF_CONJ_IN) v.im = -v.im;
+        ((C<S>*)p.x0)[2 * l] = v;
+      }
+    } else if (p.mode == BE_RADER_MID) {
+      // A = FFT(a): X[0] = x[0] + A[0] kept; then conj(A * bhat) in place
+      // (the thread that reads A[0] is the one that overwrites it)
+      C<S>* ws = (C<S>*)p.out + l * M;
+      const C<S>* __restrict__ bhat = (const C<S>*)p.bhat;
+      if (c0 == 0 && tid == 0) ((C<S>*)p.x0)[2 * l + 1] = ((C<S>*)p.x0)[2 * l] + ws[0];
+      for (uint32_t m = c0 + tid; m < c1; m += T) {
+        C<S> v = cmul(ws[m], bhat[m]);
+        v.im = -v.im;
+        ws[m] = v;
+      }
+    } else if (p.mode == BE_RADER_POST) {
+      // X[n] = x[0] + conj(y[r(n)]) for n >= 1, X[0] kept
+      const C<S>* __restrict__ ws = (const C<S>*)p.in + l * M;
+      C<S>* __restrict__ out = (C<S>*)p.out;
+      const C<S>* x0 = (const C<S>*)p.x0 + 2 * l;
+      for (uint32_t n = c0 + tid; n < c1; n += T) {
+        C<S> v;
+        if (n == 0) {
+          v = x0[1];
+        } else {
+          C<S> w = ws[p.perm_out[n - 1]];
+          w.im = -w.im;
+          v = x0[0] + w;
+        }
+        if (p.flags & PF_SCALE) v = cscale(v, sc);
+        if (p.flags & PF_CONJ_OUT) v.im = -v.im;
+        out[base + (int64_t)n * (int64_t)p.s] = v;
       }
     } else {
       const C<S>* __restrict__ ws = (const C<S>*)p.in + l * M;
@@ -687,7 +731,7 @@ cudaError_t launch_c2r_t(const RealParams& prm, unsigned grid, unsigned threads,
 }
 template <class S>
 cudaError_t launch_blue_elem_t(const BlueElemParams& prm, cudaStream_t st) {
-  const uint64_t L = prm.mode == BE_POST ? prm.N : prm.M;
+  const uint64_t L = (prm.mode == BE_POST || prm.mode == BE_RADER_POST) ? prm.N : prm.M;
   const uint64_t work = prm.nlines * ((L + kElemChunk - 1) / kElemChunk);
   uint64_t blocks = work < 148ull * 16 ? work : 148ull * 16;
   if (blocks == 0) blocks = 1;

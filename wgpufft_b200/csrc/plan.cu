@@ -474,7 +474,7 @@ struct Builder {
   // Table pointers are patched after upload, by pass index and field.
   enum Field { F_LINES_TW, F_RADER_TW, F_BLUE_TW, F_REAL_TW, F_PERM_IN, F_PERM_OUT, F_RADER_BHAT,
                F_BLUE_BHAT, F_BELEM_BHAT, F_TWS_A, F_TWS_B, F_SVOL_TW, F_BLUE_CHIRP,
-               F_BELEM_CHIRP, F_REAL_RTW };
+               F_BELEM_CHIRP, F_REAL_RTW, F_BELEM_PIN, F_BELEM_POUT, F_BELEM_X0 };
   struct Patch {
     size_t table, pass;
     Field field;
@@ -514,6 +514,9 @@ struct Builder {
         case F_BLUE_CHIRP: ps.blue.chirp = ptr; break;
         case F_BELEM_CHIRP: ps.belem.chirp = ptr; break;
         case F_REAL_RTW: ps.real.rtw = ptr; break;
+        case F_BELEM_PIN: ps.belem.perm_in = (const uint32_t*)ptr; break;
+        case F_BELEM_POUT: ps.belem.perm_out = (const uint32_t*)ptr; break;
+        case F_BELEM_X0: ps.belem.x0 = const_cast<void*>(ptr); break;
       }
     }
   }
@@ -845,6 +848,80 @@ static b2f_status add_bluestein_large(Builder& b, int axis, uint64_t N, uint64_t
   return B2F_OK;
 }
 
+// Rader for a prime p whose line does not fit one CTA, p - 1 smooth
+// (src/runtime/rader_axis.rs:1270-1286 runs long primes as multipass Rader
+// too): gather a[q] = x[g^q] into workspace lines of p - 1 points (x[0]
+// kept), FFT_{p-1} (four-step), the spectrum product (X[0] = x[0] + A[0]
+// kept), FFT_{p-1} again, and the scatter X[g^-r] = x[0] + conv[r].
+static b2f_status add_rader_large(Builder& b, int axis, uint64_t p, uint64_t s, uint64_t O,
+                                  uint32_t flags, double scale, int src, int dst) {
+  const uint64_t M = p - 1;
+  const uint64_t nlines = s * O;
+  b.need(BUF_WS2, nlines * M * b.cb());
+  b.need(dst, p * s * O * b.cb());
+  const uint64_t g = primitive_root(p);
+  const uint64_t ginv = mod_pow(g, p - 2, p);
+  std::vector<uint32_t> pin(M), pout(M);
+  std::vector<cd> bvec(M);
+  uint64_t v = 1;
+  for (uint64_t q = 0; q < M; ++q) {
+    pin[q] = (uint32_t)v;
+    v = v * g % p;
+  }
+  v = 1;
+  for (uint64_t r = 0; r < M; ++r) {
+    pout[v - 1] = (uint32_t)r;
+    bvec[r] = root_fwd(v, p);  // W_p^{g^-r}
+    v = v * ginv % p;
+  }
+  host_fft_fwd(bvec);
+  for (auto& x : bvec) x /= (double)M;
+  std::vector<unsigned char> bin(M * 4), bout(M * 4);
+  std::memcpy(bin.data(), pin.data(), bin.size());
+  std::memcpy(bout.data(), pout.data(), bout.size());
+  const size_t t_in = b.add_table(std::move(bin)), t_out = b.add_table(std::move(bout));
+  const size_t t_x0 = b.add_table(std::vector<unsigned char>(2 * nlines * b.cb(), 0));
+  const size_t t_bhat = b.add_table(b.pack_complex(bvec));
+  Pass pre;
+  pre.kind = Pass::BLUE_ELEM;
+  pre.axis = axis;
+  pre.src = src;
+  pre.dst = BUF_WS2;
+  pre.label = "rader-gather-stage";
+  pre.route = "rader";
+  pre.belem = BlueElemParams{nullptr, nullptr, nullptr, (uint32_t)p, (uint32_t)M, BE_RADER_PRE,
+                             flags & PF_CONJ_IN, s, nlines, 1.0, nullptr, nullptr, nullptr, nullptr};
+  b.set_table(b.next_pass(), Builder::F_BELEM_PIN, t_in);
+  b.set_table(b.next_pass(), Builder::F_BELEM_X0, t_x0);
+  b.plan.passes.push_back(pre);
+  int cur = BUF_WS2;
+  b2f_status st = add_complex_axis(b, axis, AxisKind::Mixed, M, 1, nlines, false, false, 1.0, &cur,
+                                   BUF_WS2, BUF_WS3, false);
+  if (st) return st;
+  Pass mid = pre;
+  mid.src = mid.dst = BUF_WS2;
+  mid.label = "rader-spectrum-product-stage";
+  mid.belem.mode = BE_RADER_MID;
+  mid.belem.flags = 0;
+  b.set_table(b.next_pass(), Builder::F_BELEM_BHAT, t_bhat);
+  b.set_table(b.next_pass(), Builder::F_BELEM_X0, t_x0);
+  b.plan.passes.push_back(mid);
+  st = add_complex_axis(b, axis, AxisKind::Mixed, M, 1, nlines, false, false, 1.0, &cur, BUF_WS2,
+                        BUF_WS3, false);
+  if (st) return st;
+  Pass post = pre;
+  post.src = BUF_WS2;
+  post.dst = dst;
+  post.label = "rader-scatter-stage";
+  post.belem.mode = BE_RADER_POST;
+  post.belem.flags = flags & (PF_CONJ_OUT | PF_SCALE);
+  post.belem.scale = scale;
+  b.set_table(b.next_pass(), Builder::F_BELEM_POUT, t_out);
+  b.set_table(b.next_pass(), Builder::F_BELEM_X0, t_x0);
+  b.plan.passes.push_back(post);
+  return B2F_OK;
+}
+
 // One complex axis of a plan: N points, stride s (complex elements), O
 // outer rows of N*s elements.  Appends one or two passes and returns the
 // buffer that holds the result.
@@ -899,6 +976,12 @@ static b2f_status add_complex_axis(Builder& b, int axis, AxisKind kind, uint64_t
         *cur = out_buf;
         return st;
       }
+    } else if (is_smooth13(N - 1)) {
+      // too long for one CTA: multipass Rader over p - 1 (half Bluestein's
+      // convolution length)
+      b2f_status st = add_rader_large(b, axis, N, s, O, flags, scale, src, out_buf);
+      if (st == B2F_OK) *cur = out_buf;
+      return st;
     }
     kind = AxisKind::Bluestein;
   }
