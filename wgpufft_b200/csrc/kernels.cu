@@ -91,9 +91,9 @@ static bool pow2_schedule_is_default(const LinesParams& prm) {
 
 cudaError_t launch_pow2(Prec p, int E, bool colmajor, const LinesParams& prm, unsigned grid,
                         unsigned threads, size_t smem, cudaStream_t st) {
-  // the compile-time kernel of this length (f32, f64) when the schedule is
-  // the one it assumes; the generic one otherwise
-  if ((p == PREC_F32 || p == PREC_F64) && pow2_schedule_is_default(prm)) {
+  // the compile-time kernel of this length when the schedule is the one it
+  // assumes; the generic one otherwise
+  if (pow2_schedule_is_default(prm)) {
     const cudaError_t e = launch_pow2_fixed(p, E, colmajor, prm, grid, threads, smem, st);
     if (e != cudaErrorInvalidValue) return e;
   }

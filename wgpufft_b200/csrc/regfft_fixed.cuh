@@ -1,5 +1,5 @@
 // Register-resident power-of-two line kernel with the line length fixed at
-// compile time (f32 and f64, N = 2^LOGN, 16 <= N <= 8192).
+// compile time (f32, f64 and df64, N = 2^LOGN, 16 <= N <= 8192).
 //
 // The same algorithm as k_pow2 (regfft.cuh): E values a thread in
 // registers, radix-16 stages then one radix 2, 4 or 8 stage, exchanges
@@ -14,6 +14,8 @@
 // generic kernel recomputes those addresses per value from runtime strides
 // (about a third of its instructions are integer addressing).
 #pragma once
+#include <type_traits>
+
 #include "regfft.cuh"
 
 namespace b2f {
@@ -114,11 +116,12 @@ FFT_D void fx_stages(cpx<S> (&v)[E], cpx<S>* line, uint32_t t, const cpx<S>* __r
 // column tiles, up to 512 otherwise).  Shared memory: G * LD values,
 // LD = N + N/16 + 1.  f32 register budgets: 64 for contiguous lines (4
 // CTAs of 256 threads per SM), 85 for 16-value column tiles (3 per SM), 128
-// for 32-value ones; f64: 128 (256 threads, 2 per SM).
+// for 32-value ones; f64 and df64: 128 (256 threads, 2 per SM).
 template <class S, int E, bool COLMAJOR>
 struct FxBounds {
-  static constexpr int threads = sizeof(S) == 8 || (COLMAJOR && E == 16) ? 256 : 512;
-  static constexpr int blocks = sizeof(S) == 8 ? 2 : (COLMAJOR ? (E == 16 ? 3 : 1) : 2);
+  static constexpr bool wide = !std::is_same<S, float>::value;  // f64, df64
+  static constexpr int threads = wide || (COLMAJOR && E == 16) ? 256 : 512;
+  static constexpr int blocks = wide ? 2 : (COLMAJOR ? (E == 16 ? 3 : 1) : 2);
 };
 template <class S, int E, bool COLMAJOR, int LOGN>
 __global__ void __launch_bounds__(FxBounds<S, E, COLMAJOR>::threads, FxBounds<S, E, COLMAJOR>::blocks)
