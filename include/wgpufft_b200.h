@@ -278,7 +278,9 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const v
  * this point).  Each of the four buffers holds `bytes` >=
  * b2f_batch_required_buffer_size_bytes; host_in == host_out and dev_in ==
  * dev_out are allowed.  Host buffers should be page-locked for the copies
- * to overlap.  Batches with cluster lines (B2F_BATCH_CLUSTERS) run
+ * to overlap.  The copies are cut at 4 KiB multiples of the buffers'
+ * offsets, so unused bytes between lines within 4 KiB of a chunk boundary
+ * are copied too (their values in host_out are unspecified).  Batches with cluster lines (B2F_BATCH_CLUSTERS) run
  * unchunked: copy in, execute, copy out. */
 b2f_status b2f_batch_execute_host(const b2f_batch* batch, void* stream, const void* host_in,
                                   void* host_out, void* dev_in, void* dev_out, uint64_t bytes);
