@@ -270,7 +270,9 @@ b2f_status b2f_batch_execute_parts(const b2f_batch* batch, void* stream, const v
                                    uint64_t in_bytes, void* out, uint64_t out_bytes,
                                    uint32_t parts, int32_t sequential);
 /* b2f_batch_execute from and to host memory: the lines are cut, in offset
- * order, into chunks of about 32 MiB (at most 32), and chunk c's copy in
+ * order, into chunks of about 32 MiB (at most 32; with 8 or more, the
+ * first three and the last three hold 1/8, 1/4 and 1/2 of the others'
+ * share, to shorten the pipeline's fill and drain), and chunk c's copy in
  * (host_in -> dev_in), transform (dev_in -> dev_out) and copy out
  * (dev_out -> host_out) overlap the other chunks' on three internal
  * streams; `stream` orders the whole call with the caller's work (the call

@@ -84,8 +84,8 @@ static uint64_t mod_pow64(uint64_t b, uint64_t e, uint64_t m) {
 }
 
 // Host-buffer execution (b2f_batch_execute_host) pipelines the lines in
-// chunks: contiguous runs of lines (in offset order) of about equal bytes,
-// about kHostChunkBytes each and at most kHostChunks, each copied in,
+// chunks: contiguous runs of lines (in offset order), about kHostChunkBytes
+// each and at most kHostChunks (smaller at both ends), each copied in,
 // transformed and copied out on its own (smaller chunks shorten the
 // pipeline's fill and drain, which are all that the copies do not hide).
 constexpr uint32_t kHostChunks = 32;
@@ -604,7 +604,10 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
     }
   }
   // chunks of host execution: lines in offset order, cut into runs of about
-  // equal bytes
+  // equal bytes, except that with 8 chunks or more the first three and the
+  // last three hold 1/8, 1/4 and 1/2 of the others' share, so that the
+  // pipeline's fill (the first copy in) and drain (the last transform and
+  // copy out) are short
   std::vector<uint32_t> chunk_of(nlines, 0);
   {
     uint64_t total = 0, acc = 0;
@@ -614,13 +617,19 @@ static b2f_status create_batch(const uint64_t* lengths, const uint64_t* offsets,
         1, std::min<uint64_t>(kHostChunks, (total * 8 + kHostChunkBytes - 1) / kHostChunkBytes));
     const uint32_t K = bp->n_chunks;
     bool seen[kHostChunks] = {};
+    uint64_t cum[kHostChunks + 1] = {};  // chunk c: acc / total in [cum[c], cum[c + 1]) / cum[K]
+    for (uint32_t c = 0; c < K; ++c) {
+      const uint32_t e = std::min(c, K - 1 - c);
+      cum[c + 1] = cum[c] + (K >= 8 && e < 3 ? 1u << e : 8u);
+    }
+    uint32_t cc = 0;
     for (uint64_t i = 0; i < nlines; ++i) {
       const uint64_t l = order[i];
-      const uint32_t c = (uint32_t)std::min<uint64_t>(K - 1, acc * K / total);
-      chunk_of[l] = c;
-      if (!seen[c]) bp->chunk_lo[c] = offsets[l];
-      seen[c] = true;
-      bp->chunk_hi[c] = offsets[l] + lengths[l];
+      while (cc + 1 < K && acc * cum[K] >= total * cum[cc + 1]) ++cc;
+      chunk_of[l] = cc;
+      if (!seen[cc]) bp->chunk_lo[cc] = offsets[l];
+      seen[cc] = true;
+      bp->chunk_hi[cc] = offsets[l] + lengths[l];
       acc += lengths[l];
     }
     // copy pieces: piece c starts at chunk c's first byte rounded down (not
