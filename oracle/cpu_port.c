@@ -1,7 +1,7 @@
 /*
  * Planned CPU FFT used as the CPU baseline of the benchmark.
  *
- * TEST/BASELINE INFRASTRUCTURE ONLY: the product never links or calls it.
+ * TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: the product never links or calls it.
  *
  * The reference's CPU backend, CpuFftPlan (src/cpu.rs:52-330), cannot be
  * built here: it sits on the third-party crates rustfft 6.4.1 and realfft

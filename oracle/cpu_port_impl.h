@@ -1,6 +1,6 @@
 /*
  * Body of the planned CPU FFT, instantiated for float and double by
- * cpu_port.c (REAL, SFX set before inclusion).  TEST/BASELINE
+ * cpu_port.c (REAL, SFX set before inclusion).  TEST AND CPU-BASELINE
  * INFRASTRUCTURE ONLY: see cpu_port.c.
  */
 #define CAT_(a, b) a##b
