@@ -324,8 +324,16 @@ __global__ void __launch_bounds__(256, FxRealBounds<S>::blocks)
   const bool valid = l0 + c < p.nlines;
   C* line = sm + c * LD;
   if (valid) {
+    // the packed line (h + 1 values): all of a thread's loads issued before
+    // its first shared-memory store, so they overlap
     const C* __restrict__ src = (const C*)p.in + (l0 + c) * (H + 1);
-    for (uint32_t k = t; k <= H; k += TL) line[pidx<PAD>(k)] = src[k];
+    C x[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) x[i] = src[t + i * TL];
+    const C xh = t == 0 ? src[H] : czero<S>();
+#pragma unroll
+    for (int i = 0; i < E; ++i) line[pidx<PAD>(t + i * TL)] = x[i];
+    if (t == 0) line[pidx<PAD>(H)] = xh;
   }
   __syncthreads();
   const C* __restrict__ rtw = (const C*)p.rtw;
