@@ -59,6 +59,54 @@ FFT_D void for_each_elem(uint32_t count, const FastDiv& dcount, uint32_t G, cons
   }
 }
 
+// Elements a thread takes at once in the batched loops: a loop that loads
+// one element and consumes it before the next keeps one global load in
+// flight per thread and waits out each one's latency.
+template <class S>
+struct BatchU {
+  static constexpr int value = sizeof(C<S>) <= 8 ? 8 : 4;
+};
+
+// for_each_elem, U elements a thread at a time: f(c, n) for all U first
+// (their global loads in flight together), then g(c, n, value) for each.
+template <int U, class V, class F, class Gf>
+FFT_D void for_each_elem_batched(uint32_t count, const FastDiv& dcount, uint32_t G,
+                                 const FastDiv& dG, bool cfirst, uint32_t tid, uint32_t T, F f,
+                                 Gf g) {
+  const uint32_t total = G * count;
+  auto split = [&](uint32_t e, uint32_t& c, uint32_t& n) {
+    if (cfirst) {
+      n = fdiv(e, dG);
+      c = e - n * G;
+    } else {
+      c = fdiv(e, dcount);
+      n = e - c * count;
+    }
+  };
+  uint32_t e = tid;
+  for (; e + (U - 1) * T < total; e += U * T) {
+    V v[U];
+    uint32_t cs[U], ns[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      split(e + u * T, cs[u], ns[u]);
+      v[u] = f(cs[u], ns[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) g(cs[u], ns[u], v[u]);
+  }
+  for (; e < total; e += T) {
+    uint32_t c, n;
+    split(e, c, n);
+    g(c, n, f(c, n));
+  }
+}
+
+template <class S>
+struct CPair {
+  C<S> a, b;
+};
+
 // Column tiles whose line count G is a power of two dividing the thread
 // count: each thread keeps one line c = tid mod G and walks its points
 // n = tid / G, + T / G, ... (no division per value, stepped addresses).
@@ -77,7 +125,19 @@ FFT_D void load_lines(C<S>* sm, const LinesParams& p, const Group& g, uint32_t t
       const int64_t es = p.io.in_es;
       const C<S>* src = in + g.in0 + (int64_t)c * g.dl_in;
       C<S>* line = sm + c * p.LD;
-      for (uint32_t n = tid >> lg; n < p.N; n += dn) {
+      constexpr int U = BatchU<S>::value;
+      uint32_t n = tid >> lg;
+      for (; n + (U - 1) * dn < p.N; n += U * dn) {
+        C<S> v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = src[(int64_t)(n + u * dn) * es];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (conj_in) v[u].im = -v[u].im;
+          line[pidx<PAD>(n + u * dn)] = v[u];
+        }
+      }
+      for (; n < p.N; n += dn) {
         C<S> v = src[(int64_t)n * es];
         if (conj_in) v.im = -v.im;
         line[pidx<PAD>(n)] = v;
@@ -85,14 +145,18 @@ FFT_D void load_lines(C<S>* sm, const LinesParams& p, const Group& g, uint32_t t
     }
     return;
   }
-  for_each_elem(p.N, p.dN, p.G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T,
-                [&](uint32_t c, uint32_t n) {
-                  if (c < g.nvalid) {
-                    C<S> v = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
-                    if (conj_in) v.im = -v.im;
-                    sm[c * p.LD + pidx<PAD>(n)] = v;
-                  }
-                });
+  for_each_elem_batched<BatchU<S>::value, C<S>>(
+      p.N, p.dN, p.G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T,
+      [&](uint32_t c, uint32_t n) {
+        return c < g.nvalid ? in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es]
+                            : czero<S>();
+      },
+      [&](uint32_t c, uint32_t n, C<S> v) {
+        if (c < g.nvalid) {
+          if (conj_in) v.im = -v.im;
+          sm[c * p.LD + pidx<PAD>(n)] = v;
+        }
+      });
 }
 
 template <class S>
@@ -118,33 +182,64 @@ FFT_D void store_lines(const C<S>* sm, const LinesParams& p, const Group& g, uin
     const uint32_t n0 = tid >> lg;
     uint32_t m32 = (uint32_t)row * n0;
     const uint32_t dm = (uint32_t)row * dn;
-    for (uint32_t n = n0; n < p.N; n += dn) {
-      C<S> v = line[pidx<PAD>(n)];
-      if (fl & PF_TW_STORE) {
-        if (step_tw) {
-          v = cmul(v, cmul(ta[m32 >> sh], tb[m32 & msk]));
-          m32 += dm;
-        } else {
-          const uint64_t m = row * (uint64_t)n;
-          v = cmul(v, ta ? tw_two_level(ta, tb, m, p.d_tws) : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
-        }
-      }
+    // twiddle W_M^{row n} of point n (its table loads)
+    auto tw_at = [&](uint32_t n, uint32_t m) -> C<S> {
+      if (step_tw) return cmul(ta[m >> sh], tb[m & msk]);
+      const uint64_t mm = row * (uint64_t)n;
+      return ta ? tw_two_level(ta, tb, mm, p.d_tws) : twiddle<S>(mm % p.tw_store_M, p.tw_store_M);
+    };
+    auto put = [&](uint32_t n, C<S> v) {
       if (fl & PF_SCALE) v = cscale(v, sc);
       if (fl & PF_CONJ_OUT) v.im = -v.im;
       dst[(int64_t)n * es] = v;
+    };
+    uint32_t n = n0;
+    if (fl & PF_TW_STORE) {
+      // U points' table loads in flight together
+      constexpr int U = BatchU<S>::value;
+      for (; n + (U - 1) * dn < p.N; n += U * dn) {
+        C<S> w[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) w[u] = tw_at(n + u * dn, m32 + u * dm);
+#pragma unroll
+        for (int u = 0; u < U; ++u) put(n + u * dn, cmul(line[pidx<PAD>(n + u * dn)], w[u]));
+        m32 += U * dm;
+      }
     }
+    for (; n < p.N; n += dn) {
+      C<S> v = line[pidx<PAD>(n)];
+      if (fl & PF_TW_STORE) {
+        v = cmul(v, tw_at(n, m32));
+        m32 += dm;
+      }
+      put(n, v);
+    }
+    return;
+  }
+  if (fl & PF_TW_STORE) {
+    // row < M / N and n < N: the exponent stays below M
+    for_each_elem_batched<BatchU<S>::value, C<S>>(
+        p.N, p.dN, p.G, p.dG, fl & PF_CFIRST_STORE, tid, T,
+        [&](uint32_t c, uint32_t n) {
+          if (c >= g.nvalid) return czero<S>();
+          const uint64_t row = fdiv((uint32_t)(g.c0 + c), p.d_tw);
+          const uint64_t m = row * (uint64_t)n;
+          return p.tws_a ? tw_two_level((const C<S>*)p.tws_a, (const C<S>*)p.tws_b, m, p.d_tws)
+                         : twiddle<S>(m % p.tw_store_M, p.tw_store_M);
+        },
+        [&](uint32_t c, uint32_t n, C<S> w) {
+          if (c < g.nvalid) {
+            C<S> v = cmul(sm[c * p.LD + pidx<PAD>(n)], w);
+            if (fl & PF_SCALE) v = cscale(v, sc);
+            if (fl & PF_CONJ_OUT) v.im = -v.im;
+            out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
+          }
+        });
     return;
   }
   for_each_elem(p.N, p.dN, p.G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t n) {
     if (c < g.nvalid) {
       C<S> v = sm[c * p.LD + pidx<PAD>(n)];
-      if (fl & PF_TW_STORE) {
-        // row < M / N and n < N: the exponent stays below M
-        const uint64_t row = fdiv((uint32_t)(g.c0 + c), p.d_tw);
-        const uint64_t m = row * (uint64_t)n;
-        v = cmul(v, p.tws_a ? tw_two_level((const C<S>*)p.tws_a, (const C<S>*)p.tws_b, m, p.d_tws)
-                            : twiddle<S>(m % p.tw_store_M, p.tw_store_M));
-      }
       if (fl & PF_SCALE) v = cscale(v, sc);
       if (fl & PF_CONJ_OUT) v.im = -v.im;
       out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
@@ -193,13 +288,9 @@ __global__ void __launch_bounds__(512) k_rader(const __grid_constant__ RaderPara
   load_lines<S>(A, p, g, tid, T);
   __syncthreads();
   if (tid < G) x0s[tid] = A[tid * LD];
-  {
-    const uint32_t tot = G * P1;
-    for (uint32_t e = tid; e < tot; e += T) {
-      const uint32_t l = fdiv(e, rp.dP1), q = e - l * P1;
-      B[l * LD + pidx<PAD>(q)] = A[l * LD + pidx<PAD>(rp.perm_in[q])];
-    }
-  }
+  for_each_elem_batched<8, uint32_t>(
+      P1, rp.dP1, G, p.dG, false, tid, T, [&](uint32_t, uint32_t q) { return rp.perm_in[q]; },
+      [&](uint32_t l, uint32_t q, uint32_t j) { B[l * LD + pidx<PAD>(q)] = A[l * LD + pidx<PAD>(j)]; });
   __syncthreads();
   C<S>* r1 = fft_lines_smem<S>(B, A, p.sch, G, LD, tid, T, tw_of<S>(p));
   C<S>* o1 = (r1 == A) ? B : A;
@@ -207,13 +298,13 @@ __global__ void __launch_bounds__(512) k_rader(const __grid_constant__ RaderPara
   __syncthreads();
   {
     const C<S>* __restrict__ bhat = (const C<S>*)rp.bhat;
-    const uint32_t tot = G * P1;
-    for (uint32_t e = tid; e < tot; e += T) {
-      const uint32_t l = fdiv(e, rp.dP1), m = e - l * P1;
-      C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], bhat[m]);
-      v.im = -v.im;
-      r1[l * LD + pidx<PAD>(m)] = v;
-    }
+    for_each_elem_batched<BatchU<S>::value, C<S>>(
+        P1, rp.dP1, G, p.dG, false, tid, T, [&](uint32_t, uint32_t m) { return bhat[m]; },
+        [&](uint32_t l, uint32_t m, C<S> b) {
+          C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], b);
+          v.im = -v.im;
+          r1[l * LD + pidx<PAD>(m)] = v;
+        });
   }
   __syncthreads();
   const C<S>* r2 = fft_lines_smem<S>(r1, o1, p.sch, G, LD, tid, T, tw_of<S>(p));
@@ -221,21 +312,24 @@ __global__ void __launch_bounds__(512) k_rader(const __grid_constant__ RaderPara
   C<S>* __restrict__ out = (C<S>*)p.out;
   const uint32_t fl = p.flags;
   const S sc = Scalar<S>::from_double(p.scale);
-  for_each_elem(P, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t n) {
-    if (c < g.nvalid) {
-      C<S> v;
-      if (n == 0) {
-        v = X0s[c];
-      } else {
-        C<S> w = r2[c * LD + pidx<PAD>(rp.perm_out[n - 1])];
-        w.im = -w.im;
-        v = x0s[c] + w;
-      }
-      if (fl & PF_SCALE) v = cscale(v, sc);
-      if (fl & PF_CONJ_OUT) v.im = -v.im;
-      out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
-    }
-  });
+  for_each_elem_batched<8, uint32_t>(
+      P, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T,
+      [&](uint32_t c, uint32_t n) { return c < g.nvalid && n > 0 ? rp.perm_out[n - 1] : 0u; },
+      [&](uint32_t c, uint32_t n, uint32_t j) {
+        if (c < g.nvalid) {
+          C<S> v;
+          if (n == 0) {
+            v = X0s[c];
+          } else {
+            C<S> w = r2[c * LD + pidx<PAD>(j)];
+            w.im = -w.im;
+            v = x0s[c] + w;
+          }
+          if (fl & PF_SCALE) v = cscale(v, sc);
+          if (fl & PF_CONJ_OUT) v.im = -v.im;
+          out[g.out0 + (int64_t)c * g.dl_out + (int64_t)n * p.io.out_es] = v;
+        }
+      });
 }
 
 // -------------------------------------------------------------- Bluestein
@@ -263,13 +357,22 @@ __global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ Blues
   {
     const C<S>* __restrict__ in = (const C<S>*)p.in;
     const bool conj_in = p.flags & PF_CONJ_IN;
-    for_each_elem(N, p.dN, G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T, [&](uint32_t c, uint32_t n) {
-      if (c < g.nvalid) {
-        C<S> v = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
-        if (conj_in) v.im = -v.im;
-        A[c * LD + pidx<PAD>(n)] = cmul(v, ctab ? ctab[n] : chirp<S>(n, N));
-      }
-    });
+    for_each_elem_batched<BatchU<S>::value, CPair<S>>(
+        N, p.dN, G, p.dG, p.flags & PF_CFIRST_LOAD, tid, T,
+        [&](uint32_t c, uint32_t n) {
+          CPair<S> x{czero<S>(), czero<S>()};
+          if (c < g.nvalid) {
+            x.a = in[g.in0 + (int64_t)c * g.dl_in + (int64_t)n * p.io.in_es];
+            x.b = ctab ? ctab[n] : chirp<S>(n, N);
+          }
+          return x;
+        },
+        [&](uint32_t c, uint32_t n, CPair<S> x) {
+          if (c < g.nvalid) {
+            if (conj_in) x.a.im = -x.a.im;
+            A[c * LD + pidx<PAD>(n)] = cmul(x.a, x.b);
+          }
+        });
     const uint32_t pad = M - N;
     const uint32_t tot = G * pad;
     for (uint32_t e = tid; e < tot; e += T) {
@@ -282,29 +385,34 @@ __global__ void __launch_bounds__(512) k_bluestein(const __grid_constant__ Blues
   C<S>* o1 = (r1 == A) ? B : A;
   {
     const C<S>* __restrict__ bhat = (const C<S>*)bp.bhat;
-    const uint32_t tot = G * M;
-    for (uint32_t e = tid; e < tot; e += T) {
-      const uint32_t l = fdiv(e, bp.dM), m = e - l * M;
-      C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], bhat[m]);
-      v.im = -v.im;
-      r1[l * LD + pidx<PAD>(m)] = v;
-    }
+    for_each_elem_batched<BatchU<S>::value, C<S>>(
+        M, bp.dM, G, p.dG, false, tid, T, [&](uint32_t, uint32_t m) { return bhat[m]; },
+        [&](uint32_t l, uint32_t m, C<S> b) {
+          C<S> v = cmul(r1[l * LD + pidx<PAD>(m)], b);
+          v.im = -v.im;
+          r1[l * LD + pidx<PAD>(m)] = v;
+        });
   }
   __syncthreads();
   const C<S>* r2 = fft_lines_smem<S>(r1, o1, p.sch, G, LD, tid, T, tw_of<S>(p));
   C<S>* __restrict__ out = (C<S>*)p.out;
   const uint32_t fl = p.flags;
   const S sc = Scalar<S>::from_double(p.scale);
-  for_each_elem(N, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T, [&](uint32_t c, uint32_t k) {
-    if (c < g.nvalid) {
-      C<S> w = r2[c * LD + pidx<PAD>(k)];
-      w.im = -w.im;
-      C<S> v = cmul(w, ctab ? ctab[k] : chirp<S>(k, N));
-      if (fl & PF_SCALE) v = cscale(v, sc);
-      if (fl & PF_CONJ_OUT) v.im = -v.im;
-      out[g.out0 + (int64_t)c * g.dl_out + (int64_t)k * p.io.out_es] = v;
-    }
-  });
+  for_each_elem_batched<BatchU<S>::value, C<S>>(
+      N, p.dN, G, p.dG, fl & PF_CFIRST_STORE, tid, T,
+      [&](uint32_t c, uint32_t k) {
+        return c < g.nvalid ? (ctab ? ctab[k] : chirp<S>(k, N)) : czero<S>();
+      },
+      [&](uint32_t c, uint32_t k, C<S> ch) {
+        if (c < g.nvalid) {
+          C<S> w = r2[c * LD + pidx<PAD>(k)];
+          w.im = -w.im;
+          C<S> v = cmul(w, ch);
+          if (fl & PF_SCALE) v = cscale(v, sc);
+          if (fl & PF_CONJ_OUT) v.im = -v.im;
+          out[g.out0 + (int64_t)c * g.dl_out + (int64_t)k * p.io.out_es] = v;
+        }
+      });
 }
 
 // ------------------------------------------------------------------ real
