@@ -255,10 +255,24 @@ FFT_D c32* ilv_fft(c32* a, c32* b, const LongSched& sch, uint32_t lg, uint32_t t
   return a;
 }
 
+// x mod m for x < 2^50, m < 2^32, inv = 1/m rounded to double: the
+// quotient estimate trunc(x * inv) is off by at most one (its relative
+// error is below 2^-51, x / m below 2^50), so one correction either way
+// gives the remainder.  A 64-bit integer modulo is a long software routine
+// on the GPU; this is a few instructions.
+FFT_D uint32_t mod_u50(uint64_t x, uint32_t m, double inv) {
+  const uint64_t q = (uint64_t)((double)x * inv);
+  int64_t r = (int64_t)x - (int64_t)(q * m);
+  if (r < 0) r += m;
+  else if (r >= (int64_t)m) r -= m;
+  return (uint32_t)r;
+}
+
 // Chirp exp(-i pi n^2 / N) at n, n + D, n + 2D, ... : q = n^2 mod 2N kept
 // incrementally ((n + D)^2 = n^2 + 2nD + D^2); W_2N^q from the length's
 // two-level chirp table (q = a B + b: ca[a] * cb[b]), read through the
 // read-only cache (value_ldg) or from a shared-memory copy (value).
+// n < 2^24 and D < 2^24 (the residues below need n^2, 2nD, 2D^2 < 2^50).
 struct ChirpWalk {
   uint32_t q, u, dsq, u2, twoN, sh, mask;
   const c32* ca;
@@ -270,10 +284,11 @@ struct ChirpWalk {
     sh = split;
     mask = (1u << split) - 1;
     twoN = 2 * N;
-    q = (uint32_t)((n * n) % twoN);
-    u = (uint32_t)((2 * n * (uint64_t)D) % twoN);
-    dsq = (uint32_t)(((uint64_t)D * D) % twoN);
-    u2 = (uint32_t)((2 * (uint64_t)D * D) % twoN);
+    const double inv = 1.0 / (double)twoN;
+    q = mod_u50(n * n, twoN, inv);
+    u = mod_u50(2 * n * (uint64_t)D, twoN, inv);
+    dsq = mod_u50((uint64_t)D * D, twoN, inv);
+    u2 = mod_u50(2 * (uint64_t)D * D, twoN, inv);
   }
   FFT_D void step() {
     q += u;
@@ -385,12 +400,32 @@ FFT_D void long_compute(const LongParams& p, const LongLenDesc& d, const LongTas
       ChirpWalk cw;
       cw.init(n, S * N2, d.N, p.tw + d.ca, p.tw + d.cb, d.csplit);
       c32* dp = X + i0 * P + l;
-      for (uint32_t i = i0; i < N1 && n < d.N; i += S) {
+      const uint32_t dn = S * N2;
+      uint32_t i = i0;
+      // four chirp values' loads in flight together
+      constexpr int U = 4;
+      for (; i + (U - 1) * S < N1 && n + (U - 1) * dn < d.N; i += U * S) {
+        c32 w[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          w[u] = cw.value_ldg();
+          cw.step();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          c32 v = dp[u * S * P];
+          if (inv) v.im = -v.im;
+          dp[u * S * P] = cmul(v, w[u]);
+        }
+        n += U * dn;
+        dp += U * S * P;
+      }
+      for (; i < N1 && n < d.N; i += S) {
         c32 v = *dp;
         if (inv) v.im = -v.im;
         *dp = cmul(v, cw.value_ldg());
         cw.step();
-        n += S * N2;
+        n += dn;
         dp += S * P;
       }
     }
