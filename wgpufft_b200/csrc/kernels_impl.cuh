@@ -432,9 +432,12 @@ __global__ void __launch_bounds__(512) k_r2c_even(const __grid_constant__ RealPa
   const uint64_t l0 = (uint64_t)blockIdx.x * G;
   const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
   const C<S>* __restrict__ in = (const C<S>*)p.in;
-  for_each_elem(h, p.dh, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t n) {
-    if (c < nvalid) A[c * LD + pidx<PAD>(n)] = in[(l0 + c) * h + n];
-  });
+  for_each_elem_batched<4, C<S>>(
+      h, p.dh, G, p.dG, false, tid, T,
+      [&](uint32_t c, uint32_t n) { return c < nvalid ? in[(l0 + c) * h + n] : czero<S>(); },
+      [&](uint32_t c, uint32_t n, C<S> v) {
+        if (c < nvalid) A[c * LD + pidx<PAD>(n)] = v;
+      });
   __syncthreads();
   const C<S>* Z = fft_lines_smem<S>(A, B, p.sch, G, LD, tid, T,
                                      (p.flags & PF_TW_TABLE) ? (const C<S>*)p.tw : nullptr);
@@ -478,9 +481,12 @@ __global__ void __launch_bounds__(512) k_c2r_even(const __grid_constant__ RealPa
   const uint64_t l0 = (uint64_t)blockIdx.x * G;
   const uint32_t nvalid = (p.nlines - l0) < G ? (uint32_t)(p.nlines - l0) : G;
   const C<S>* __restrict__ in = (const C<S>*)p.in;
-  for_each_elem(P, p.dP, G, p.dG, false, tid, T, [&](uint32_t c, uint32_t k) {
-    if (c < nvalid) A[c * LD + pidx<PAD>(k)] = in[(l0 + c) * P + k];
-  });
+  for_each_elem_batched<4, C<S>>(
+      P, p.dP, G, p.dG, false, tid, T,
+      [&](uint32_t c, uint32_t k) { return c < nvalid ? in[(l0 + c) * P + k] : czero<S>(); },
+      [&](uint32_t c, uint32_t k, C<S> v) {
+        if (c < nvalid) A[c * LD + pidx<PAD>(k)] = v;
+      });
   __syncthreads();
   {
     const uint32_t K = h / 2 + 1;
