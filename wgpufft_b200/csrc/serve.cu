@@ -201,6 +201,8 @@ struct Server {
     return used + plan_bytes + registry_bytes() + need <= budget;
   }
 
+  std::unique_lock<std::mutex>* run_lock = nullptr;  // the scheduler thread's hold on mu
+
   // The resident plan of cfg (a batch bucket or an exact batch), created when new.
   SPlan* get_plan(const Config& cfg, int32_t kind, b2f_status* st) {
     const std::string k = config_key(cfg, kind) + "|b" + std::to_string(cfg.batch);
@@ -211,8 +213,13 @@ struct Server {
       it->second.lru = std::prev(lru.end());
       return &it->second;
     }
+    // built with the lock released (tables and workspace take allocations
+    // and uploads): submitters and waiters are not held up meanwhile; only
+    // this thread touches the plan map
     Plan* p = nullptr;
+    if (run_lock) run_lock->unlock();
     *st = create_plan(cfg, kind, device, &p);
+    if (run_lock) run_lock->lock();
     if (*st) return nullptr;
     SPlan& sp = plans[k];
     sp.plan.reset(p);
@@ -457,6 +464,7 @@ struct Server {
   void run() {
     cudaSetDevice(device);
     std::unique_lock<std::mutex> lk(mu);
+    run_lock = &lk;
     while (true) {
       // wake for new work at once; with groups in flight, poll their
       // completion every 20 us with the lock released (submitters and
