@@ -301,7 +301,9 @@ b2f_status b2f_batch_diagnostics_json(const b2f_batch* batch, char* buf, uint64_
  * resident plan (plans keyed by configuration and a power-of-two batch
  * bucket, or by the exact batch once a batch recurs; evicted least recently
  * used when the budget needs the room).  A lone 1D request runs on a plan.
- * Requests carry host buffers (pinned memory lets the copies overlap;
+ * Plans are built on the scheduler thread with its lock released, so
+ * submits and waits never stall behind a build; the group that needs the
+ * plan waits for it.  Requests carry host buffers (pinned memory lets the copies overlap;
  * results are written back to host_out) or device buffers
  * (b2f_server_submit_device).  When a group fails, no copy touching a
  * request's memory is pending by the time its wait returns the error.
